@@ -1,0 +1,346 @@
+"""Benchmark: adjoint-mode circuit gradients at n = 26 (the headline metric).
+
+Workload (one "step" = one full energy + gradient evaluation):
+  26 qubits, FP32 amplitudes with FP64 accumulation; 20 layers of RX, RY, RZ
+  on every qubit plus CRX(i, i+1) for i = 1..25 (2,060 parameters, uniform in
+  [0, 2 pi), seeded); observable = open-chain XXZ, sum X_iX_{i+1} + Y_iY_{i+1}
+  + 0.5 Z_iZ_{i+1} (75 Pauli terms); psi0 = |0...0>.
+
+Arms:
+  default            this engine (libvqcb200, sm_100a) through its C ABI;
+  --impl reference   the reference's algorithm on the host cores (the C++
+                     restatement under oracle/, all host threads), on a
+                     bounded sample of the same workload scaled to grads/s.
+
+Multi-GPU (torchrun): every rank runs an independent replica (the path has no
+exchange step at this size); value = sum over ranks of grads/s, timed as the
+max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "vqc.jl_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+N_QUBITS = 26
+LAYERS = 20
+SEED = 20261203
+METRIC = "circuit grads/s at n=26 (FP32 states, FP64 accumulation)"
+UNIT = "grads/s"
+
+
+def workload():
+    from vqcb200 import workloads as W
+    rng = np.random.default_rng(SEED)
+    theta = rng.uniform(0, 2 * np.pi, LAYERS * (4 * N_QUBITS - 1))
+    spec = W.rxyz_crx_spec(N_QUBITS, LAYERS, theta)
+    hspec = W.xxz_spec(N_QUBITS, 0.5)
+    return spec, hspec
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_id), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 8:
+                    continue
+                try:
+                    sm.append(float(f[0]))
+                    smax.append(float(f[1]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[4:8]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_from_profiles(kernel):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(REPO, "profiles", "ncu_traffic.json")) as f:
+            d = json.load(f)
+        return d.get(kernel, {}).get("dram_bytes_per_launch_full_size")
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------------------- CPU arm
+def cpu_sample(nthreads, reps=1, n=N_QUBITS, dtype=np.complex64):
+    """Times the oracle's restatement of the reference's gradient on a bounded
+    sample of the workload and scales it to one full gradient.
+
+    Sample: forward + reverse sweep (uncompute of both states, one two-state
+    expectation pass per parameter: circuitdiff.jl:23-32) of 2 single-qubit
+    rotations and 1 CRX at full n, plus one XXZ key (expectation + the two
+    H-apply passes of the expectation pullback); scaled by the workload's
+    counts: 20 x (78 rotations + 25 CRX) gates and 25 keys."""
+    from oracle import oracle as O
+    spec, hspec = workload()
+    psi = O.zero_state(n, dtype)
+    O.apply_gate(psi, [0], np.array([[1, 1], [1, -1]]) / np.sqrt(2), nthreads)  # a dense-ish start
+    lam = psi.copy()
+    sample_1q = [g for g in O.from_spec(spec[:3])][:2]
+    sample_crx = O.from_spec([s for s in spec if s[0] == "crx"][:1])
+
+    def sweep(gates):
+        t0 = time.perf_counter()
+        for pos, U, _ in gates:
+            O.apply_gate(psi, pos, U, nthreads)
+        for pos, U, dUs in reversed(gates):
+            Ud = U.conj().T
+            O.apply_gate(lam, pos, Ud, nthreads)
+            O.apply_gate(psi, pos, Ud, nthreads)
+            for dU in dUs:
+                O.expect_dense(lam, pos, dU.conj().T @ U, vc=psi, nthreads=nthreads)
+        return time.perf_counter() - t0
+
+    t1 = sum(sweep(sample_1q) for _ in range(reps)) / (reps * len(sample_1q))
+    tc = sum(sweep(sample_crx) for _ in range(reps)) / reps
+    key = O.group_by_key(O.terms_from_spec(hspec[:3]))
+    (kpos, kM), = key.items()
+    t0 = time.perf_counter()
+    O.expect_dense(psi, kpos, kM.astype(dtype), nthreads=nthreads)
+    out = np.zeros_like(psi)
+    O.apply_gate_add(psi, out, kpos, kM, nthreads)
+    O.apply_gate_add(psi, out, kpos, kM.conj().T, nthreads)
+    tk = time.perf_counter() - t0
+    per_grad = LAYERS * (3 * n * t1 + (n - 1) * tc) + (n - 1) * tk
+    sample_s = reps * (2 * t1 + tc) + tk
+    return 1.0 / per_grad, sample_s
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(nthreads)
+    vals, secs = [], 0.0
+    for _ in range(args.steps):
+        v, s = cpu_sample(nthreads)
+        vals.append(v)
+        secs += s
+    value = float(np.median(vals))
+    sample = ("per step: 2 rotations + 1 CRX forward and reverse sweep and one XXZ key at n=26, FP32 amplitudes "
+              "(the reference's ComplexF32 path, FP32 accumulation), scaled to 20x(78 rotations + 25 CRX) + 25 keys")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic (seeded)", "config": config_dict(args),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    return {"workload": "adjoint gradient, n=26, 20 x (RX,RY,RZ on every qubit + CRX(i,i+1)), XXZ 75 terms",
+            "n_qubits": N_QUBITS, "layers": LAYERS, "n_params": LAYERS * (4 * N_QUBITS - 1), "n_pauli_terms": 75,
+            "state_bytes": (1 << N_QUBITS) * 8, "l2": "state (512 MiB) larger than L2; no flush needed",
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import vqcb200 as V
+    from vqcb200 import _lib
+    from vqcb200 import workloads as W
+    from vqcb200.circuit import Packed
+
+    torch.cuda.set_device(local_rank)
+    lib = V.load()
+    spec, hspec = workload()
+    circuit = W.to_circuit(spec)
+    H = W.to_operator(hspec)
+    packed = Packed(circuit)
+    terms, nterms = H.packed()
+
+    def make_state(dtype):
+        return V.StateVector(N_QUBITS, dtype=dtype, device=local_rank)
+
+    def grad_call(psi0, grads, energy):
+        _lib.check(lib.vqc_adjoint_grad(psi0.handle, packed.gates, packed.ngates, packed.mats_ptr(), packed.params,
+                                        packed.nparams, terms, nterms, energy, grads.ctypes.data_as(_lib._D)))
+
+    def timed(psi0, steps, warmup, profile=False, e2e_host=None):
+        grads = np.zeros(packed.nparams)
+        energy = (ctypes.c_double * 2)()
+        stream = torch.cuda.ExternalStream(lib.vqc_state_stream(psi0.handle), device=local_rank)
+        for _ in range(warmup):
+            if e2e_host is not None:
+                psi0.upload(e2e_host)
+                V.energy_and_gradient(H, circuit, psi0)
+            else:
+                grad_call(psi0, grads, energy)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        if profile:
+            _lib.profile_enable(True)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            if e2e_host is not None:
+                _lib.check(lib.vqc_state_upload(psi0.handle, ctypes.c_void_p(e2e_host.data_ptr()),
+                                                e2e_host.numel() * e2e_host.element_size()))
+                e, g = V.energy_and_gradient(H, circuit, psi0)
+            else:
+                grad_call(psi0, grads, energy)
+        end.record(stream)
+        end.synchronize()
+        torch.cuda.synchronize()
+        prof = None
+        if profile:
+            prof = _lib.profile_read()
+            _lib.profile_enable(False)
+        ms = start.elapsed_time(end) / steps
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            torch.distributed.barrier()
+            ms = float(t.item())
+        return ms, prof, complex(energy[0], energy[1]), grads
+
+    psi32 = make_state(np.complex64)
+    try:
+        gpu_id = torch.cuda.get_device_properties(local_rank).uuid
+        gpu_id = "GPU-" + str(gpu_id) if not str(gpu_id).startswith("GPU-") else str(gpu_id)
+    except Exception:
+        gpu_id = local_rank
+    clocks = Clocks(gpu_id)
+    clocks.start()
+    ms, prof, energy, grads = timed(psi32, args.steps, args.warmup, profile=True)
+    clk = clocks.stop()
+    value = world * 1000.0 / ms
+
+    # end to end through the public API with psi0 in pinned host memory
+    host = torch.zeros(2 << N_QUBITS, dtype=torch.float32).pin_memory()
+    host[0] = 1.0
+    ms_e2e, _, _, _ = timed(psi32, max(1, args.steps // 2), 1, e2e_host=host)
+
+    # the plain FP64 path, for the FP32-vs-FP64 speedup
+    psi64 = make_state(np.complex128)
+    ms64, _, energy64, grads64 = timed(psi64, max(1, args.steps // 2), 1)
+    del psi64
+
+    if rank != 0:
+        return
+    hbm, peak_kind = peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    launches = sum(v[0] for v in prof.values()) if prof else 0
+    if dom:
+        name, (n, tot_ms, tot_bytes) = dom
+        achieved = tot_bytes / (tot_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                "bytes_per_launch": tot_bytes / n, "avg_launch_ms": tot_ms / n,
+                "share_of_step": tot_ms / (ms * args.steps), "traffic": traffic_from_profiles(name)}
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        v, s = cpu_sample(nthreads, reps=8)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": "8 x (2 rotations + 1 CRX forward/reverse sweep) + one XXZ key at n=26, FP32, scaled "
+                         "to one gradient (%.1f s of CPU work)" % s}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded angles, |0> input)",
+            "config": config_dict(args),
+            "e2e": {"value": world * 1000.0 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": (1 << N_QUBITS) * 8,
+                    "d2h_bytes_per_step": packed.nparams * 8 + 16},
+            "fp64_plain": {"value": world * 1000.0 / ms64, "unit": UNIT, "ms_per_step": ms64,
+                           "fp32_speedup": ms64 / ms,
+                           "energy_rel_diff_fp32_vs_fp64": abs(energy - energy64) / abs(energy64),
+                           "grad_rel_diff_fp32_vs_fp64": float(np.linalg.norm(grads - grads64) / np.linalg.norm(grads64))},
+            "energy": energy.real,
+            "roofline": roof, "kernels": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in (prof or {}).items()},
+            "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

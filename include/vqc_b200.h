@@ -1,0 +1,177 @@
+/*
+ * vqc_b200.h -- C ABI of libvqcb200.so, the B200 (sm_100a) engine for the
+ * state-vector hot path of guochu/VQC.jl.
+ *
+ * Each entry point replaces one Julia method of the reference (cited as
+ * file:line within the VQC.jl project).  The Julia side binds them with
+ * `ccall` (vqc.jl_b200/julia/VQCB200.jl); the Python host mirror binds them
+ * with ctypes (vqc.jl_b200/vqcb200/_lib.py).
+ *
+ * Conventions, identical to the reference:
+ *   - qubits are 0-based here (1-based in Julia): qubit q <-> bit q of the
+ *     amplitude index, least significant first (statevector.jl:167-176);
+ *   - a k-qubit matrix is row-major 2^k x 2^k, complex interleaved (re, im)
+ *     FP64; bit b of its row/column index <-> pos[b], in the order given
+ *     (QuantumCircuits' ordered_mat is applied inside);
+ *   - a density matrix of n qubits is stored as a 2n-qubit vector: bits
+ *     0..n-1 index the row, bits n..2n-1 the column (densitymatrix.jl:27-30);
+ *   - amplitudes are complex interleaved, FP32 (VQC_C64) or FP64 (VQC_C128);
+ *     every norm, inner product, expectation and gradient is accumulated in
+ *     FP64 on the device and returned as FP64.
+ *
+ * Every function returns 0 (VQC_OK) or a negative status; vqc_last_error()
+ * gives the message of the last failure on the calling thread.  A handle owns
+ * one CUDA stream; calls on one handle are serialised, calls on different
+ * handles may run concurrently from different threads.  Calls that return a
+ * host value synchronise the handle's stream; the others are asynchronous
+ * unless stated.
+ */
+#ifndef VQC_B200_H
+#define VQC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VQC_OK 0
+#define VQC_ERR_ARG (-1)         /* bad argument (throw/@assert/ArgumentError in the reference) */
+#define VQC_ERR_OOM (-2)         /* device allocation failed */
+#define VQC_ERR_CUDA (-3)        /* CUDA runtime error */
+#define VQC_ERR_UNSUPPORTED (-4) /* e.g. a >5-qubit gate (generic.jl:37) */
+#define VQC_ERR_TIMEOUT (-5)     /* a bounded wait ran out (serving) */
+#define VQC_ERR_BUSY (-6)        /* serving: no slot or memory free for the request now */
+
+#define VQC_C64 0  /* ComplexF32 amplitudes */
+#define VQC_C128 1 /* ComplexF64 amplitudes */
+
+typedef struct vqc_state_s* vqc_state;
+
+/* One gate of a circuit: nq positions, its matrix at mats + mat (in doubles). */
+typedef struct {
+  int32_t nq;
+  int32_t pos[5];
+  int64_t mat;
+} vqc_gate;
+
+/* One circuit parameter: derivative dU/dtheta of gate `gate`, at mats + dmat. */
+typedef struct {
+  int32_t gate;
+  int32_t reserved;
+  int64_t dmat;
+} vqc_param;
+
+/* One Pauli string coeff * prod_q P_q, P_q = I, X, Z, Y for (x_q, z_q) =
+ * (0,0), (1,0), (0,1), (1,1): x bit q of xmask, z bit q of zmask. */
+typedef struct {
+  uint64_t xmask;
+  uint64_t zmask;
+  double coeff_re;
+  double coeff_im;
+} vqc_pauli;
+
+const char* vqc_last_error(void);
+const char* vqc_version(void);
+/* Number of CUDA devices visible, or a negative status. */
+int vqc_device_count(void);
+
+/* ---- state vectors: StateVector{T} (statevector.jl:1-21) ------------------ */
+/* StateVector(T, n): |0...0> on `device` (statevector.jl:15-21). */
+int vqc_state_create(int n, int dtype, int device, vqc_state* out);
+int vqc_state_destroy(vqc_state h);
+int vqc_state_nqubits(vqc_state h);  /* stored qubits: 2n for a density matrix */
+int vqc_state_dtype(vqc_state h);
+/* storage(x) copies (statevector.jl:24): bytes must equal 2^nq * amplitude size. */
+int vqc_state_upload(vqc_state h, const void* host, size_t bytes);
+int vqc_state_download(vqc_state h, void* host, size_t bytes);
+/* reset!(x) (statevector.jl:110-114): |0...0>, or |0><0| for a density matrix. */
+int vqc_state_reset(vqc_state h);
+/* copy(x) (statevector.jl:30): same qubit count; converts FP32 <-> FP64. */
+int vqc_state_copy(vqc_state dst, vqc_state src);
+/* norm(x) (statevector.jl:53), FP64. */
+int vqc_state_norm(vqc_state h, double* out);
+/* dot(x, y) = <x|y> (statevector.jl:54), FP64; out = (re, im). */
+int vqc_state_dot(vqc_state x, vqc_state y, double* out);
+/* Block the caller until the handle's queued work is done. */
+int vqc_state_sync(vqc_state h);
+/* Device pointer of the amplitudes (for interop; owned by the handle). */
+void* vqc_state_device_ptr(vqc_state h);
+/* The handle's cudaStream_t (for interop and event timing). */
+void* vqc_state_stream(vqc_state h);
+
+/* ---- launch profiling (no counterpart in the reference) -------------------
+ * vqc_profile_enable(1) clears the records and starts timing every kernel
+ * launch with CUDA events on its stream, per kernel class; (0) stops.  Each
+ * class reports launches, total device ms and total algorithmic bytes (the
+ * bytes the operation must move at minimum). */
+int vqc_profile_enable(int on);
+int vqc_profile_count(void);
+int vqc_profile_get(int i, char* name, int name_len, long long* launches, double* total_ms, double* total_bytes);
+
+/* ---- gates: apply!(::Gate, ::StateVector) (applygates/generic/generic.jl:6-14,
+ *      _apply_gate_threaded2! in threaded_short_range.jl / threaded_long_range.jl,
+ *      specialised kernels in the applygates/specific directory) ------------- */
+int vqc_apply_gate(vqc_state h, int k, const int* pos, const double* mat);
+/* apply!(::QCircuit, state) (generic.jl:26-31).  fuse != 0 plans the gates
+ * into shared-memory tile passes (one HBM round trip per pass); fuse == 0
+ * applies them one by one, like the reference. */
+int vqc_apply_circuit(vqc_state h, const vqc_gate* gates, int ngates, const double* mats, int fuse);
+
+/* ---- expectation (hamiltonian/expecs/expecs.jl:12-78) --------------------- */
+/* expectation(H, psi) for a Pauli sum; out = (re, im) in FP64. */
+int vqc_expect_pauli(vqc_state psi, const vqc_pauli* terms, int nterms, double* out);
+/* expectation(phi, H, psi) = <phi|H|psi> (expecs.jl:45-74, expec_threaded_2.jl). */
+int vqc_expect_pauli2(vqc_state phi, vqc_state psi, const vqc_pauli* terms, int nterms, double* out);
+/* expectation_value(pos, M, psi[, phi]) for one dense k<=5-qubit key
+ * (expecs.jl:85-130); phi may be NULL for the one-state form. */
+int vqc_expect_dense(vqc_state phi, vqc_state psi, int k, const int* pos, const double* mat, double* out);
+
+/* ---- H * psi (hamiltonian/apply_qterms/apply_qterms.jl:13-28) ------------- */
+/* out = H psi for a Pauli sum (out is overwritten). */
+int vqc_apply_pauli(vqc_state psi, vqc_state out, const vqc_pauli* terms, int nterms);
+/* out += M psi on pos for one dense key (short_range_threaded.jl:1519-1524). */
+int vqc_apply_dense_add(vqc_state psi, vqc_state out, int k, const int* pos, const double* mat);
+
+/* ---- gradients: the Zygote adjoints of *(circuit, psi) (circuitdiff.jl:2-8,
+ *      23-32, 61-78) and of expectation(H, psi) (expecdiff.jl:30-33, 68) ------ */
+/* Energy and gradient of real(expectation(H, circuit(theta) * psi0)):
+ * forward pass, E = <y|H|y>, cotangent (H + H^dagger) y, then the reverse
+ * sweep that uncomputes the forward state instead of storing it.  psi0 is not
+ * modified.  grads[j] is dE/dtheta_j for params[j] (any order).  energy =
+ * (re, im).  Blocks until the result is on the host. */
+int vqc_adjoint_grad(vqc_state psi0, const vqc_gate* gates, int ngates, const double* mats,
+                     const vqc_param* params, int nparams, const vqc_pauli* terms, int nterms, double* energy,
+                     double* grads);
+/* The circuit pullback alone (back_propagate, circuitdiff.jl:61-75): given the
+ * output state y = circuit * psi0 and the cotangent delta of a real loss,
+ * overwrite y with psi0 (uncomputed) and delta with the input cotangent, and
+ * return grads[j] = Re <delta_out | dU/dtheta_j | y_in> for params[j]. */
+int vqc_circuit_backward(vqc_state y, vqc_state delta, const vqc_gate* gates, int ngates, const double* mats,
+                         const vqc_param* params, int nparams, double* grads);
+
+/* ---- density matrices (densitymatrix.jl, generic.jl:16-24, 54-64,
+ *      ptrace.jl:4-53, measure.jl:69-81) ------------------------------------ */
+/* DensityMatrix(T, n): |0><0|, stored as a 2n-qubit vector (4^n amplitudes). */
+int vqc_dm_create(int n, int dtype, int device, vqc_state* out);
+int vqc_dm_nqubits(vqc_state rho);
+/* DensityMatrix(psi) = |psi><psi| (densitymatrix.jl:27); psi has n qubits. */
+int vqc_dm_from_state(vqc_state rho, vqc_state psi);
+/* apply!(::Gate, ::DensityMatrix): rho <- U rho U^dagger.  The reference runs
+ * U on the row qubits and conj(U) on the column qubits in two passes; here
+ * both act in one pass. */
+int vqc_dm_apply_gate(vqc_state rho, int k, const int* pos, const double* mat);
+int vqc_dm_apply_circuit(vqc_state rho, const vqc_gate* gates, int ngates, const double* mats, int fuse);
+/* partial_tr(rho, sites): out (host) receives the 2^(n-m) x 2^(n-m) result,
+ * column-major, complex FP64 interleaved; the kept qubits keep their order. */
+int vqc_dm_ptrace(vqc_state rho, int nsites, const int* sites, double* out);
+/* real(diag(rho)): out (host) receives 2^n FP64 probabilities. */
+int vqc_dm_probs(vqc_state rho, double* out);
+/* tr(rho) (densitymatrix.jl:58), FP64 (re, im). */
+int vqc_dm_trace(vqc_state rho, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VQC_B200_H */

@@ -1,0 +1,270 @@
+// Adjoint-mode circuit gradients: the Zygote adjoint of *(circuit, psi)
+// (circuitdiff.jl:2-8, back_propagate :23-32, back_propagate_util :61-75)
+// and of expectation(H, psi) (expecdiff.jl:30-33, 68).
+//
+// Reverse sweep, per gate (last to first), as the reference does:
+//   delta <- U^dagger delta,  y <- U^dagger y          (uncompute, no storage)
+//   grad_j = Re <delta_out | dU/dtheta_j | y_in>
+//          = Re sum_ab D_j[a,b] A[a,b],  D_j = U^dagger dU/dtheta_j,
+//            A[a,b] = sum over groups of conj(delta_a) y_b   (after the uncompute)
+// The reference evaluates one two-state expectation pass per parameter
+// (real(expectation(y, dG, delta)), circuitdiff.jl:29).  Here the uncompute of
+// both states and the reduced matrix A are one pass: A is accumulated in FP64
+// over the gate's active subspace (D_j vanishes outside it), reduced on the
+// device in a fixed order, and the per-parameter contractions with D_j run on
+// the host in FP64.
+#include <algorithm>
+#include <cstring>
+
+#include "engine.h"
+#include "subspace.cuh"
+
+namespace vqc {
+
+int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vqc_pauli* terms, int nterms,
+              bool write, bool acc, bool hermitian_part, double* result);
+int expect_dense_device(vqc_state h, const void* bra, const void* ket, int k, const int* sp, const std::vector<cd>& M,
+                        double* res);
+int apply_circuit_raw(vqc_state h, const vqc_gate* gates, int ngates, const double* mats, bool dm, int fuse);
+
+constexpr int kAccMaxS = 4;  // A is reduced in one pass for |S| <= 4
+
+// lam, psi <- U^dagger (a.U holds U^dagger restricted to S); with ACC,
+// out (device) receives A[a][b] = sum conj(lam_a) psi_b as (re, im) pairs.
+template <class R, int MS, bool ACC>
+__global__ void __launch_bounds__(kRedThreads)
+    k_adjoint_sub(cplx<R>* __restrict__ lam, cplx<R>* __restrict__ psi, const __grid_constant__ SubArgs<R, MS> a,
+                  Scratch s, double* out) {
+  double acc[ACC ? 2 * MS * MS : 1];
+#pragma unroll
+  for (int i = 0; i < (ACC ? 2 * MS * MS : 1); ++i) acc[i] = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ngroups; g += stride) {
+    const int64_t base = group_base(g, a.k, a.mask);
+    cplx<R> xl[MS], xp[MS], yl[MS], yp[MS];
+#pragma unroll
+    for (int s = 0; s < MS; ++s)
+      if (s < a.ns) {
+        xl[s] = lam[base + a.off[s]];
+        xp[s] = psi[base + a.off[s]];
+      }
+#pragma unroll
+    for (int r = 0; r < MS; ++r) {
+      if (r < a.ns) {
+        cplx<R> al = mkc<R>(R(0), R(0)), ap = al;
+#pragma unroll
+        for (int c = 0; c < MS; ++c)
+          if (c < a.ns) {
+            al = cfma(a.U[r * MS + c], xl[c], al);
+            ap = cfma(a.U[r * MS + c], xp[c], ap);
+          }
+        yl[r] = al;
+        yp[r] = ap;
+        lam[base + a.off[r]] = al;
+        psi[base + a.off[r]] = ap;
+      }
+    }
+    if (ACC) {
+#pragma unroll
+      for (int r = 0; r < MS; ++r) {
+        if (r < a.ns) {
+          const double2 l = to_d2(yl[r]);
+#pragma unroll
+          for (int c = 0; c < MS; ++c)
+            if (c < a.ns) {
+              const double2 p = to_d2(yp[c]);
+              double* q = &acc[2 * (r * MS + c)];
+              q[0] = fma(l.x, p.x, fma(l.y, p.y, q[0]));
+              q[1] = fma(l.x, p.y, fma(-l.y, p.x, q[1]));
+            }
+        }
+      }
+    }
+  }
+  if (ACC) grid_reduce<(ACC ? 2 * MS * MS : 1)>(acc, s, out);
+}
+
+template <class R, int MS>
+static int launch_adj(const GateSpec& gd, vqc_state h, void* lam, void* psi, bool acc, double* out) {
+  SubArgs<R, MS> a;
+  fill_sub_args<R, MS>(gd, h->nq, a);
+  if (gd.mode != kDense) {  // the kernel is written for the dense form: expand
+    for (int i = 0; i < MS * MS; ++i) a.U[i] = mkc<R>(R(0), R(0));
+    for (int r = 0; r < gd.ns; ++r)
+      for (int c = 0; c < gd.ns; ++c) {
+        cd u = gd.US[r * gd.ns + c];
+        a.U[r * MS + c] = mkc<R>((R)u.real(), (R)u.imag());
+      }
+  }
+  const int grid = acc ? reduction_grid(h->device, a.ngroups) : launch_grid(h->device, a.ngroups);
+  ProfScope prof(h->stream, "adjoint_gate", 4.0 * a.ngroups * gd.ns * sizeof(cplx<R>));
+  if constexpr (MS <= kAccMaxS) {
+    if (acc) {
+      k_adjoint_sub<R, MS, true><<<grid, kRedThreads, 0, h->stream>>>((cplx<R>*)lam, (cplx<R>*)psi, a, h->scr, out);
+      VQC_CK(cudaGetLastError());
+      return VQC_OK;
+    }
+  }
+  k_adjoint_sub<R, MS, false><<<grid, kRedThreads, 0, h->stream>>>((cplx<R>*)lam, (cplx<R>*)psi, a, h->scr, out);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+template <class R>
+static int launch_adj_r(const GateSpec& gd, vqc_state h, void* lam, void* psi, bool acc, double* out) {
+  switch (ms_of(gd.ns)) {
+    case 1: return launch_adj<R, 1>(gd, h, lam, psi, acc, out);
+    case 2: return launch_adj<R, 2>(gd, h, lam, psi, acc, out);
+    case 4: return launch_adj<R, 4>(gd, h, lam, psi, acc, out);
+    case 8: return launch_adj<R, 8>(gd, h, lam, psi, false, out);
+    case 16: return launch_adj<R, 16>(gd, h, lam, psi, false, out);
+    default: return launch_adj<R, 32>(gd, h, lam, psi, false, out);
+  }
+}
+
+struct ParamRef {
+  int index;  // position in the caller's params array
+  std::vector<cd> D;  // U^dagger dU/dtheta in sorted order (2^k x 2^k)
+};
+
+// The reverse sweep over lam (cotangent) and y (state): both are overwritten
+// with their values at the circuit input; grads[j] receive the partials.
+static int reverse_sweep(vqc_state h, void* lam, void* y, const vqc_gate* gates, int ngates, const double* mats,
+                         const vqc_param* params, int nparams, double* grads) {
+  if (nparams < 0 || (nparams > 0 && (!params || !grads))) return fail(VQC_ERR_ARG, "bad parameter arrays");
+  std::vector<std::vector<ParamRef>> per_gate(ngates);
+  for (int j = 0; j < nparams; ++j) {
+    const int gi = params[j].gate;
+    if (gi < 0 || gi >= ngates) return fail(VQC_ERR_ARG, "parameter refers to a gate out of range");
+    per_gate[gi].push_back(ParamRef{j, {}});
+  }
+  // device rows for A, one per gate with parameters and |S| <= kAccMaxS
+  int rows = 0;
+  std::vector<int> row_of(ngates, -1);
+  std::vector<GateSpec> specs(ngates);
+  for (int i = 0; i < ngates; ++i) {
+    const vqc_gate& gt = gates[i];
+    int rc = analyze_gate(h->nq, gt.nq, gt.pos, mats + gt.mat, true, specs[i]);
+    if (rc) return rc;
+    if (!per_gate[i].empty()) {
+      // D_j = U^dagger dU_j, both in sorted order
+      const GateSpec& gs = specs[i];
+      const int d = 1 << gs.k;
+      for (ParamRef& pr : per_gate[i]) {
+        int sp[5];
+        std::vector<cd> dU;
+        if ((rc = order_matrix(h->nq, gt.nq, gt.pos, mats + params[pr.index].dmat, sp, dU))) return rc;
+        pr.D.assign((size_t)d * d, cd(0));
+        for (int r = 0; r < d; ++r)
+          for (int c = 0; c < d; ++c) {
+            cd acc = 0;
+            for (int m = 0; m < d; ++m) acc += gs.U[(size_t)r * d + m] * dU[(size_t)m * d + c];  // gs.U = U^dagger
+            pr.D[(size_t)r * d + c] = acc;
+          }
+      }
+      if (specs[i].ns <= kAccMaxS) row_of[i] = rows++;
+    }
+  }
+  if ((size_t)rows > h->accbuf_rows) {
+    if (h->accbuf) {
+      VQC_CK(cudaStreamSynchronize(h->stream));
+      VQC_CK(cudaFree(h->accbuf));
+      h->accbuf = nullptr;
+    }
+    VQC_CK(cudaMalloc(&h->accbuf, sizeof(double) * 2 * kAccMaxS * kAccMaxS * std::max(rows, 1)));
+    h->accbuf_rows = std::max(rows, 1);
+  }
+  // gates with |S| > kAccMaxS and parameters: one two-state pass per parameter
+  for (int i = ngates - 1; i >= 0; --i) {
+    const GateSpec& gs = specs[i];
+    const bool acc = row_of[i] >= 0;
+    double* out = acc ? h->accbuf + (size_t)row_of[i] * 2 * kAccMaxS * kAccMaxS : nullptr;
+    int rc = VQC_OK;
+    if (gs.ns > 0)
+      rc = h->dtype == VQC_C64 ? launch_adj_r<float>(gs, h, lam, y, acc, out)
+                               : launch_adj_r<double>(gs, h, lam, y, acc, out);
+    else if (acc) {
+      // identity gate (e.g. a rotation by 0): A over an empty subspace is unusable,
+      // fall back to direct passes below
+      row_of[i] = -1;
+    }
+    if (rc) return rc;
+    if (!per_gate[i].empty() && row_of[i] < 0) {
+      for (const ParamRef& pr : per_gate[i]) {
+        if ((rc = expect_dense_device(h, lam, y, gs.k, gs.sp, pr.D, h->scr.result))) return rc;
+        if ((rc = fetch_result(h, 2))) return rc;
+        grads[pr.index] = h->h_result[0];
+      }
+    }
+  }
+  if (rows > 0) {
+    std::vector<double> A((size_t)rows * 2 * kAccMaxS * kAccMaxS);
+    VQC_CK(cudaMemcpyAsync(A.data(), h->accbuf, sizeof(double) * A.size(), cudaMemcpyDeviceToHost, h->stream));
+    VQC_CK(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < ngates; ++i) {
+      if (row_of[i] < 0) continue;
+      const GateSpec& gs = specs[i];
+      const int d = 1 << gs.k, MS = ms_of(gs.ns);
+      const double* a = &A[(size_t)row_of[i] * 2 * kAccMaxS * kAccMaxS];
+      for (const ParamRef& pr : per_gate[i]) {
+        double g = 0;
+        for (int r = 0; r < gs.ns; ++r)
+          for (int c = 0; c < gs.ns; ++c) {
+            const cd Dv = pr.D[(size_t)gs.S[r] * d + gs.S[c]];
+            const cd Av(a[2 * (r * MS + c)], a[2 * (r * MS + c) + 1]);
+            g += (Dv * Av).real();
+          }
+        grads[pr.index] = g;
+      }
+    }
+  } else {
+    VQC_CK(cudaStreamSynchronize(h->stream));
+  }
+  return VQC_OK;
+}
+
+}  // namespace vqc
+
+using namespace vqc;
+
+extern "C" {
+
+int vqc_adjoint_grad(vqc_state psi0, const vqc_gate* gates, int ngates, const double* mats, const vqc_param* params,
+                     int nparams, const vqc_pauli* terms, int nterms, double* energy, double* grads) {
+  int rc = enter(psi0);
+  if (rc) return rc;
+  if (psi0->n_dm) return fail(VQC_ERR_ARG, "adjoint gradient of a density matrix is not on this path");
+  if (!energy) return fail(VQC_ERR_ARG, "null energy output");
+  if (ngates < 0 || (ngates > 0 && (!gates || !mats))) return fail(VQC_ERR_ARG, "bad circuit arrays");
+  std::lock_guard<std::mutex> lk(psi0->mu);
+  void* w[2];
+  if ((rc = workspace(psi0, 2, w))) return rc;
+  void* y = w[0];
+  void* lam = w[1];
+  VQC_CK(cudaMemcpyAsync(y, psi0->d, psi0->size() * psi0->amp_bytes(), cudaMemcpyDeviceToDevice, psi0->stream));
+  // forward: y = circuit * psi0 (run on a view of psi0's handle whose buffer is y)
+  void* keep = psi0->d;
+  psi0->d = y;
+  rc = apply_circuit_raw(psi0, gates, ngates, mats, false, 1);
+  psi0->d = keep;
+  if (rc) return rc;
+  // E = <y|H|y>; cotangent lam = (conj(z) H + z H^dagger) y with z = 1
+  if ((rc = pauli_run(psi0, y, y, lam, terms, nterms, true, true, true, energy))) return rc;
+  return reverse_sweep(psi0, lam, y, gates, ngates, mats, params, nparams, grads);
+}
+
+int vqc_circuit_backward(vqc_state y, vqc_state delta, const vqc_gate* gates, int ngates, const double* mats,
+                         const vqc_param* params, int nparams, double* grads) {
+  int rc = enter(y);
+  if (rc) return rc;
+  if (!delta || delta == y || delta->nq != y->nq || delta->dtype != y->dtype || delta->device != y->device ||
+      y->n_dm || delta->n_dm)
+    return fail(VQC_ERR_ARG, "backward: y and delta must be distinct state vectors of one size, dtype and device");
+  if (ngates < 0 || (ngates > 0 && (!gates || !mats))) return fail(VQC_ERR_ARG, "bad circuit arrays");
+  std::lock_guard<std::mutex> lk(y->mu);
+  if ((rc = stream_after(y, delta))) return rc;
+  if ((rc = reverse_sweep(y, delta->d, y->d, gates, ngates, mats, params, nparams, grads))) return rc;
+  return stream_after(delta, y);
+}
+
+}  // extern "C"

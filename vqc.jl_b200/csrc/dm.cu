@@ -1,0 +1,223 @@
+// Density matrices: DensityMatrix{T} (densitymatrix.jl:1-30), the unitary
+// gate rho <- U rho U^dagger (applygates/generic/generic.jl:16-24, 54-64),
+// partial_tr (ptrace.jl:4-53), basis probabilities (measure.jl:69-81;
+// real(diag(storage(rho)))) and tr (densitymatrix.jl:58).
+//
+// rho of n qubits is the 2n-qubit vector of its column-major storage: bit q
+// (q < n) of the flat index is row qubit q, bit n + q is column qubit q.
+// The reference applies U on the row qubits and conj(U) on the column qubits
+// in two passes; for k <= 2 this file applies W = conj(U) (x) U on the 2k
+// positions (pos, pos + n) in ONE pass (half the HBM traffic), and in two
+// passes for k >= 3 (W would exceed the 5-qubit kernel limit).
+#include <algorithm>
+
+#include "engine.h"
+#include "subspace.cuh"
+
+namespace vqc {
+
+int dm_apply_gate_raw(vqc_state h, int k, const int* pos, const double* mat) {
+  const int n = h->n_dm;
+  if (k < 1) return fail(VQC_ERR_ARG, "gate needs at least one position");
+  if (k > 5) return fail(VQC_ERR_UNSUPPORTED, "only implement 5-qubit gates and less currently.");
+  if (!pos || !mat) return fail(VQC_ERR_ARG, "null positions or matrix");
+  for (int i = 0; i < k; ++i)
+    if (pos[i] < 0 || pos[i] >= n) return fail(VQC_ERR_ARG, "gate position out of range");
+  const int d = 1 << k;
+  if (2 * k <= 5) {
+    const int D = d * d;
+    std::vector<double> W((size_t)2 * D * D);
+    for (int r2 = 0; r2 < d; ++r2)
+      for (int r1 = 0; r1 < d; ++r1)
+        for (int c2 = 0; c2 < d; ++c2)
+          for (int c1 = 0; c1 < d; ++c1) {
+            const cd u(mat[2 * (r1 * d + c1)], mat[2 * (r1 * d + c1) + 1]);
+            const cd v(mat[2 * (r2 * d + c2)], mat[2 * (r2 * d + c2) + 1]);
+            const cd w = u * std::conj(v);
+            const size_t idx = (size_t)(r1 + d * r2) * D + (c1 + d * c2);
+            W[2 * idx] = w.real();
+            W[2 * idx + 1] = w.imag();
+          }
+    int p2[10];
+    for (int i = 0; i < k; ++i) {
+      p2[i] = pos[i];
+      p2[k + i] = pos[i] + n;
+    }
+    return apply_gate_raw(h, 2 * k, p2, W.data());
+  }
+  int rc = apply_gate_raw(h, k, pos, mat);
+  if (rc) return rc;
+  std::vector<double> Uc((size_t)2 * d * d);
+  for (size_t i = 0; i < (size_t)d * d; ++i) {
+    Uc[2 * i] = mat[2 * i];
+    Uc[2 * i + 1] = -mat[2 * i + 1];
+  }
+  int p2[5];
+  for (int i = 0; i < k; ++i) p2[i] = pos[i] + n;
+  return apply_gate_raw(h, k, p2, Uc.data());
+}
+
+// rho[r + L c] = psi[r] conj(psi[c])
+template <class R>
+__global__ void k_dm_from_state(cplx<R>* rho, const cplx<R>* psi, int n) {
+  const int64_t L = int64_t(1) << n, N = L * L;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const cplx<R> a = psi[i & (L - 1)], b = psi[i >> n];
+    rho[i] = mkc<R>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+  }
+}
+
+// deposit the low bits of v into the set bits of mask
+__device__ __forceinline__ int64_t deposit(int64_t v, uint64_t mask) {
+  int64_t r = 0;
+  while (mask) {
+    const uint64_t low = mask & (~mask + 1);
+    if (v & 1) r |= (int64_t)low;
+    v >>= 1;
+    mask ^= low;
+  }
+  return r;
+}
+
+// out[a + s1 b] = sum_c rho[(K(a)|T(c)) + L (K(b)|T(c))], FP64 accumulation.
+template <class R>
+__global__ void k_dm_ptrace(const cplx<R>* __restrict__ rho, int n, uint64_t kept, uint64_t traced, int nk, int nt,
+                            double2* __restrict__ out) {
+  const int64_t L = int64_t(1) << n, s1 = int64_t(1) << nk, s2 = int64_t(1) << nt;
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < s1 * s1; o += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = o & (s1 - 1), b = o >> nk;
+    const int64_t ra = deposit(a, kept), cb = deposit(b, kept);
+    double2 acc = make_double2(0, 0);
+    for (int64_t c = 0; c < s2; ++c) {
+      const int64_t t = deposit(c, traced);
+      const double2 v = to_d2(rho[(ra | t) + L * (cb | t)]);
+      acc.x += v.x;
+      acc.y += v.y;
+    }
+    out[o] = acc;
+  }
+}
+
+template <class R>
+__global__ void k_dm_diag(const cplx<R>* __restrict__ rho, int n, double* __restrict__ out) {
+  const int64_t L = int64_t(1) << n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)rho[i + L * i].x;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kRedThreads) k_dm_trace(const cplx<R>* __restrict__ rho, int n, Scratch s) {
+  const int64_t L = int64_t(1) << n;
+  double acc[2] = {0, 0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = to_d2(rho[i + L * i]);
+    acc[0] += v.x;
+    acc[1] += v.y;
+  }
+  grid_reduce<2>(acc, s, s.result);
+}
+
+}  // namespace vqc
+
+using namespace vqc;
+
+extern "C" {
+
+int vqc_dm_from_state(vqc_state rho, vqc_state psi) {
+  int rc = enter(rho);
+  if (rc) return rc;
+  if (!rho->n_dm || !psi || psi->n_dm || psi->nq != rho->n_dm || psi->dtype != rho->dtype || psi->device != rho->device)
+    return fail(VQC_ERR_ARG, "DensityMatrix(psi): shapes, dtypes or devices differ");
+  std::lock_guard<std::mutex> lk(rho->mu);
+  if ((rc = stream_after(rho, psi))) return rc;
+  const int g = launch_grid(rho->device, rho->size());
+  if (rho->dtype == VQC_C64)
+    k_dm_from_state<float><<<g, 256, 0, rho->stream>>>((float2*)rho->d, (const float2*)psi->d, rho->n_dm);
+  else
+    k_dm_from_state<double><<<g, 256, 0, rho->stream>>>((double2*)rho->d, (const double2*)psi->d, rho->n_dm);
+  VQC_CK(cudaGetLastError());
+  return stream_after(psi, rho);
+}
+
+int vqc_dm_apply_gate(vqc_state rho, int k, const int* pos, const double* mat) {
+  int rc = enter(rho);
+  if (rc) return rc;
+  if (!rho->n_dm) return fail(VQC_ERR_ARG, "not a density matrix");
+  std::lock_guard<std::mutex> lk(rho->mu);
+  return dm_apply_gate_raw(rho, k, pos, mat);
+}
+
+int vqc_dm_ptrace(vqc_state rho, int nsites, const int* sites, double* out) {
+  int rc = enter(rho);
+  if (rc) return rc;
+  const int n = rho->n_dm;
+  if (!n) return fail(VQC_ERR_ARG, "not a density matrix");
+  if (!out || nsites < 0 || nsites > n || (nsites > 0 && !sites)) return fail(VQC_ERR_ARG, "bad sites");
+  uint64_t traced = 0;
+  for (int i = 0; i < nsites; ++i) {
+    if (sites[i] < 0 || sites[i] >= n) return fail(VQC_ERR_ARG, "site out of range.");
+    if (traced >> sites[i] & 1) return fail(VQC_ERR_ARG, "duplicate sites not allowed.");
+    traced |= 1ull << sites[i];
+  }
+  const uint64_t kept = ((n >= 64) ? ~0ull : ((1ull << n) - 1)) & ~traced;
+  const int nk = n - nsites;
+  const int64_t s1 = int64_t(1) << nk;
+  std::lock_guard<std::mutex> lk(rho->mu);
+  double2* dout = nullptr;
+  VQC_CK(cudaMallocAsync((void**)&dout, sizeof(double2) * s1 * s1, rho->stream));
+  const int g = launch_grid(rho->device, s1 * s1);
+  if (rho->dtype == VQC_C64)
+    k_dm_ptrace<float><<<g, 256, 0, rho->stream>>>((const float2*)rho->d, n, kept, traced, nk, nsites, dout);
+  else
+    k_dm_ptrace<double><<<g, 256, 0, rho->stream>>>((const double2*)rho->d, n, kept, traced, nk, nsites, dout);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, dout, sizeof(double2) * s1 * s1, cudaMemcpyDeviceToHost, rho->stream);
+  cudaFreeAsync(dout, rho->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(rho->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "partial trace");
+  return VQC_OK;
+}
+
+int vqc_dm_probs(vqc_state rho, double* out) {
+  int rc = enter(rho);
+  if (rc) return rc;
+  const int n = rho->n_dm;
+  if (!n) return fail(VQC_ERR_ARG, "not a density matrix");
+  if (!out) return fail(VQC_ERR_ARG, "null output");
+  std::lock_guard<std::mutex> lk(rho->mu);
+  const int64_t L = int64_t(1) << n;
+  double* dout = nullptr;
+  VQC_CK(cudaMallocAsync((void**)&dout, sizeof(double) * L, rho->stream));
+  const int g = launch_grid(rho->device, L);
+  if (rho->dtype == VQC_C64)
+    k_dm_diag<float><<<g, 256, 0, rho->stream>>>((const float2*)rho->d, n, dout);
+  else
+    k_dm_diag<double><<<g, 256, 0, rho->stream>>>((const double2*)rho->d, n, dout);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, sizeof(double) * L, cudaMemcpyDeviceToHost, rho->stream);
+  cudaFreeAsync(dout, rho->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(rho->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "probabilities");
+  return VQC_OK;
+}
+
+int vqc_dm_trace(vqc_state rho, double* out) {
+  int rc = enter(rho);
+  if (rc) return rc;
+  if (!rho->n_dm) return fail(VQC_ERR_ARG, "not a density matrix");
+  if (!out) return fail(VQC_ERR_ARG, "null output");
+  std::lock_guard<std::mutex> lk(rho->mu);
+  const int g = reduction_grid(rho->device, int64_t(1) << rho->n_dm);
+  if (rho->dtype == VQC_C64)
+    k_dm_trace<float><<<g, kRedThreads, 0, rho->stream>>>((const float2*)rho->d, rho->n_dm, rho->scr);
+  else
+    k_dm_trace<double><<<g, kRedThreads, 0, rho->stream>>>((const double2*)rho->d, rho->n_dm, rho->scr);
+  VQC_CK(cudaGetLastError());
+  if ((rc = fetch_result(rho, 2))) return rc;
+  out[0] = rho->h_result[0];
+  out[1] = rho->h_result[1];
+  return VQC_OK;
+}
+
+}  // extern "C"

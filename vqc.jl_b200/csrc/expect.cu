@@ -1,0 +1,371 @@
+// expectation(H, psi), expectation(phi, H, psi) and H * psi on the device.
+//
+// Reference: hamiltonian/expecs/expecs.jl:12-78 (one pass per position key,
+// accumulation in eltype(psi)), expec_threaded.jl / expec_threaded_2.jl (the
+// loops), apply_qterms/apply_qterms.jl:13-28 and short_range_threaded.jl
+// (vout += M_key psi per key).
+//
+// Pauli sums take one pass over the state for the whole operator: terms are
+// grouped by their X/Y flip mask x; for output index i each group reads the
+// partner amplitude psi[i ^ x] once and multiplies it by the group's summed
+// phase f_x(i) = sum_t c_t i^{|x & z_t|} (-1)^{|(i ^ x) & z_t|}.  All sums are
+// FP64 (also for FP32 states) and reduced in a fixed order.
+#include <algorithm>
+#include <cstring>
+#include <map>
+
+#include "engine.h"
+#include "subspace.cuh"
+
+namespace vqc {
+
+struct DevTerm {
+  uint64_t z;
+  double2 c;  // coefficient for the expectation, times i^{popcount(x & z)}
+  double2 d;  // coefficient for the applied operator, same phase
+};
+struct DevGroup {
+  uint64_t x;
+  int start, count;
+};
+
+constexpr int kMaxTermsPerLaunch = 2048;
+
+// Prepared operator: groups + terms, uploaded to h->opbuf.
+struct PauliPlan {
+  std::vector<DevGroup> groups;
+  std::vector<DevTerm> terms;
+};
+
+static int plan_pauli(int nq, const vqc_pauli* t, int nt, bool apply_hermitian_part, PauliPlan& p) {
+  if (nt < 0 || (nt > 0 && !t)) return fail(VQC_ERR_ARG, "bad Pauli term array");
+  const uint64_t lim = nq >= 64 ? ~0ull : ((1ull << nq) - 1);
+  std::map<uint64_t, std::vector<int>> by_x;
+  for (int i = 0; i < nt; ++i) {
+    if ((t[i].xmask & ~lim) || (t[i].zmask & ~lim)) return fail(VQC_ERR_ARG, "Pauli term acts outside the register");
+    by_x[t[i].xmask].push_back(i);
+  }
+  for (auto& kv : by_x) {
+    DevGroup g{kv.first, (int)p.terms.size(), (int)kv.second.size()};
+    for (int i : kv.second) {
+      const int ny = __builtin_popcountll(t[i].xmask & t[i].zmask) & 3;
+      const cd ph[4] = {cd(1, 0), cd(0, 1), cd(-1, 0), cd(0, -1)};
+      cd c = cd(t[i].coeff_re, t[i].coeff_im) * ph[ny];
+      // (H + H^dagger): a Pauli string is Hermitian, so its coefficient becomes 2 Re(c).
+      cd d = apply_hermitian_part ? cd(2 * t[i].coeff_re, 0) * ph[ny] : c;
+      p.terms.push_back(DevTerm{t[i].zmask, make_double2(c.real(), c.imag()), make_double2(d.real(), d.imag())});
+    }
+    p.groups.push_back(g);
+  }
+  return VQC_OK;
+}
+
+// One pass: optionally out = H' psi, and sum conj(bra_i) (H psi)_i.
+template <class R, bool WRITE, bool ACC>
+__global__ void __launch_bounds__(kRedThreads)
+    k_pauli(const cplx<R>* __restrict__ bra, const cplx<R>* __restrict__ ket, cplx<R>* __restrict__ out, int64_t N,
+            const DevGroup* __restrict__ groups, int ng, const DevTerm* __restrict__ terms, int nt, Scratch s,
+            double* res) {
+  extern __shared__ unsigned char smem[];
+  DevGroup* sg = reinterpret_cast<DevGroup*>(smem);
+  DevTerm* st = reinterpret_cast<DevTerm*>(smem + sizeof(DevGroup) * ng);
+  for (int i = threadIdx.x; i < ng; i += blockDim.x) sg[i] = groups[i];
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) st[i] = terms[i];
+  __syncthreads();
+  double acc[2] = {0, 0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += stride) {
+    double2 hv = make_double2(0, 0), ov = make_double2(0, 0);
+    for (int gi = 0; gi < ng; ++gi) {
+      const DevGroup g = sg[gi];
+      const int64_t j = i ^ (int64_t)g.x;
+      const double2 kv = to_d2(ket[j]);
+      double2 f = make_double2(0, 0), fd = make_double2(0, 0);
+      for (int q = g.start; q < g.start + g.count; ++q) {
+        const double sgn = (__popcll((unsigned long long)j & st[q].z) & 1) ? -1.0 : 1.0;
+        if (ACC) {
+          f.x = fma(sgn, st[q].c.x, f.x);
+          f.y = fma(sgn, st[q].c.y, f.y);
+        }
+        if (WRITE) {
+          fd.x = fma(sgn, st[q].d.x, fd.x);
+          fd.y = fma(sgn, st[q].d.y, fd.y);
+        }
+      }
+      if (ACC) hv = cfma(f, kv, hv);
+      if (WRITE) ov = cfma(fd, kv, ov);
+    }
+    if (WRITE) out[i] = mkc<R>((R)ov.x, (R)ov.y);
+    if (ACC) {
+      const double2 b = to_d2(bra[i]);
+      acc[0] = fma(b.x, hv.x, fma(b.y, hv.y, acc[0]));
+      acc[1] = fma(b.x, hv.y, fma(-b.y, hv.x, acc[1]));
+    }
+  }
+  if (ACC) grid_reduce<2>(acc, s, res);
+}
+
+template <class R>
+__global__ void k_axpy(cplx<R>* y, const cplx<R>* x, int64_t N) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    cplx<R> a = y[i], b = x[i];
+    y[i] = mkc<R>(a.x + b.x, a.y + b.y);
+  }
+}
+
+int axpy_device(vqc_state h, void* y, const void* x) {
+  const int g = launch_grid(h->device, h->size());
+  if (h->dtype == VQC_C64)
+    k_axpy<float><<<g, 256, 0, h->stream>>>((float2*)y, (const float2*)x, h->size());
+  else
+    k_axpy<double><<<g, 256, 0, h->stream>>>((double2*)y, (const double2*)x, h->size());
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+// Runs the Pauli kernel in chunks of at most kMaxTermsPerLaunch terms; the
+// expectation (if any) is summed on the host in FP64 over chunks.
+int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vqc_pauli* terms, int nterms,
+              bool write, bool acc, bool hermitian_part, double* result) {
+  double tot[2] = {0, 0};
+  bool first = true;
+  int start = 0;
+  do {
+    const int cnt = std::min(kMaxTermsPerLaunch, nterms - start);
+    PauliPlan p;
+    int rc = plan_pauli(h->nq, terms + start, cnt, hermitian_part, p);
+    if (rc) return rc;
+    if (p.groups.empty()) {
+      // empty operator: H psi = 0
+      if (write && first) VQC_CK(cudaMemsetAsync(out, 0, h->size() * h->amp_bytes(), h->stream));
+      break;
+    }
+    const size_t gb = sizeof(DevGroup) * p.groups.size(), tb = sizeof(DevTerm) * p.terms.size();
+    std::vector<unsigned char> buf(gb + tb);
+    std::memcpy(buf.data(), p.groups.data(), gb);
+    std::memcpy(buf.data() + gb, p.terms.data(), tb);
+    if ((rc = upload_ops(h, buf.data(), buf.size()))) return rc;
+    const DevGroup* dg = (const DevGroup*)h->opbuf;
+    const DevTerm* dt = (const DevTerm*)((unsigned char*)h->opbuf + gb);
+    const int ng = (int)p.groups.size(), nt = (int)p.terms.size();
+    const size_t smem = gb + tb;
+    const int grid = reduction_grid(h->device, h->size());
+    // a later chunk accumulates onto `out`: run it into a workspace and add
+    void* target = out;
+    if (write && !first) {  // the third workspace is never an operand of this call
+      void* w3[3];
+      if ((rc = workspace(h, 3, w3))) return rc;
+      target = w3[2];
+    }
+    ProfScope prof(h->stream, write ? "pauli_apply" : "pauli_expect",
+                   (double)h->size() * h->amp_bytes() * (1 + (write ? 1 : 0) + (acc && bra != ket ? 1 : 0)));
+#define VQC_PAULI_LAUNCH(R)                                                                                      \
+  do {                                                                                                           \
+    auto kfun = write ? (acc ? k_pauli<R, true, true> : k_pauli<R, true, false>)                                 \
+                      : k_pauli<R, false, true>;                                                                 \
+    if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kfun<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,     \
+                                                  h->size(), dg, ng, dt, nt, h->scr, h->scr.result);             \
+  } while (0)
+    if (h->dtype == VQC_C64)
+      VQC_PAULI_LAUNCH(float);
+    else
+      VQC_PAULI_LAUNCH(double);
+#undef VQC_PAULI_LAUNCH
+    VQC_CK(cudaGetLastError());
+    if (write && !first) {
+      if ((rc = axpy_device(h, out, target))) return rc;
+    }
+    if (acc) {
+      if ((rc = fetch_result(h, 2))) return rc;
+      tot[0] += h->h_result[0];
+      tot[1] += h->h_result[1];
+    }
+    first = false;
+    start += cnt;
+  } while (start < nterms);
+  if (result) {
+    result[0] = tot[0];
+    result[1] = tot[1];
+  }
+  return VQC_OK;
+}
+
+// ----------------------------------------------------------------------------- dense keys
+template <int MS>
+struct DenseArgs {
+  int64_t ngroups;
+  int64_t mask[6];
+  int k;
+  int64_t off[MS];
+  double2 M[MS * MS];
+};
+
+template <class R, int MS>
+__global__ void __launch_bounds__(kRedThreads)
+    k_expect_dense(const cplx<R>* __restrict__ bra, const cplx<R>* __restrict__ ket,
+                   const __grid_constant__ DenseArgs<MS> a, Scratch s, double* res) {
+  double acc[2] = {0, 0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ngroups; g += stride) {
+    const int64_t base = group_base(g, a.k, a.mask);
+    double2 x[MS];
+#pragma unroll
+    for (int c = 0; c < MS; ++c) x[c] = to_d2(ket[base + a.off[c]]);
+#pragma unroll
+    for (int r = 0; r < MS; ++r) {
+      double2 row = make_double2(0, 0);
+#pragma unroll
+      for (int c = 0; c < MS; ++c) row = cfma(a.M[r * MS + c], x[c], row);
+      const double2 b = to_d2(bra[base + a.off[r]]);
+      acc[0] = fma(b.x, row.x, fma(b.y, row.y, acc[0]));
+      acc[1] = fma(b.x, row.y, fma(-b.y, row.x, acc[1]));
+    }
+  }
+  grid_reduce<2>(acc, s, res);
+}
+
+template <class R, int MS>
+__global__ void __launch_bounds__(256)
+    k_apply_dense_add(const cplx<R>* __restrict__ ket, cplx<R>* __restrict__ out, const __grid_constant__ DenseArgs<MS> a) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ngroups; g += stride) {
+    const int64_t base = group_base(g, a.k, a.mask);
+    double2 x[MS];
+#pragma unroll
+    for (int c = 0; c < MS; ++c) x[c] = to_d2(ket[base + a.off[c]]);
+#pragma unroll
+    for (int r = 0; r < MS; ++r) {
+      double2 row = to_d2(out[base + a.off[r]]);
+#pragma unroll
+      for (int c = 0; c < MS; ++c) row = cfma(a.M[r * MS + c], x[c], row);
+      out[base + a.off[r]] = mkc<R>((R)row.x, (R)row.y);
+    }
+  }
+}
+
+template <int MS>
+static void fill_dense(int nq, int k, const int* sp, const std::vector<cd>& M, DenseArgs<MS>& a) {
+  a.ngroups = mask_of(k, sp, nq, a.mask);
+  for (int j = k + 1; j < 6; ++j) a.mask[j] = 0;
+  a.k = k;
+  for (int j = 0; j < MS; ++j) a.off[j] = offset_of(j, k, sp);
+  for (int i = 0; i < MS * MS; ++i) a.M[i] = make_double2(M[i].real(), M[i].imag());
+}
+
+template <int MS>
+static int expect_dense_ms(vqc_state h, const void* bra, const void* ket, int k, const int* sp,
+                           const std::vector<cd>& M, double* res) {
+  DenseArgs<MS> a;
+  fill_dense<MS>(h->nq, k, sp, M, a);
+  const int grid = reduction_grid(h->device, a.ngroups);
+  ProfScope prof(h->stream, "expect_dense", (double)h->size() * h->amp_bytes() * (bra == ket ? 1 : 2));
+  if (h->dtype == VQC_C64)
+    k_expect_dense<float, MS><<<grid, kRedThreads, 0, h->stream>>>((const float2*)bra, (const float2*)ket, a, h->scr, res);
+  else
+    k_expect_dense<double, MS><<<grid, kRedThreads, 0, h->stream>>>((const double2*)bra, (const double2*)ket, a, h->scr,
+                                                                    res);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+// sum conj(bra) M ket over the key's groups into res[0..1] (device).
+int expect_dense_device(vqc_state h, const void* bra, const void* ket, int k, const int* sp, const std::vector<cd>& M,
+                        double* res) {
+  switch (k) {
+    case 1: return expect_dense_ms<2>(h, bra, ket, k, sp, M, res);
+    case 2: return expect_dense_ms<4>(h, bra, ket, k, sp, M, res);
+    case 3: return expect_dense_ms<8>(h, bra, ket, k, sp, M, res);
+    case 4: return expect_dense_ms<16>(h, bra, ket, k, sp, M, res);
+    default: return expect_dense_ms<32>(h, bra, ket, k, sp, M, res);
+  }
+}
+
+template <int MS>
+static int apply_dense_ms(vqc_state h, const void* ket, void* out, int k, const int* sp, const std::vector<cd>& M) {
+  DenseArgs<MS> a;
+  fill_dense<MS>(h->nq, k, sp, M, a);
+  const int grid = launch_grid(h->device, a.ngroups);
+  if (h->dtype == VQC_C64)
+    k_apply_dense_add<float, MS><<<grid, 256, 0, h->stream>>>((const float2*)ket, (float2*)out, a);
+  else
+    k_apply_dense_add<double, MS><<<grid, 256, 0, h->stream>>>((const double2*)ket, (double2*)out, a);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+}  // namespace vqc
+
+using namespace vqc;
+
+extern "C" {
+
+int vqc_expect_pauli(vqc_state psi, const vqc_pauli* terms, int nterms, double* out) {
+  int rc = enter(psi);
+  if (rc) return rc;
+  if (!out) return fail(VQC_ERR_ARG, "null output");
+  std::lock_guard<std::mutex> lk(psi->mu);
+  return pauli_run(psi, psi->d, psi->d, nullptr, terms, nterms, false, true, false, out);
+}
+
+int vqc_expect_pauli2(vqc_state phi, vqc_state psi, const vqc_pauli* terms, int nterms, double* out) {
+  int rc = enter(psi);
+  if (rc) return rc;
+  if (!phi || !out || phi->nq != psi->nq || phi->dtype != psi->dtype || phi->device != psi->device)
+    return fail(VQC_ERR_ARG, "expectation: states differ in size, dtype or device");
+  std::lock_guard<std::mutex> lk(psi->mu);
+  if ((rc = stream_after(psi, phi))) return rc;
+  return pauli_run(psi, phi->d, psi->d, nullptr, terms, nterms, false, true, false, out);
+}
+
+int vqc_apply_pauli(vqc_state psi, vqc_state out, const vqc_pauli* terms, int nterms) {
+  int rc = enter(psi);
+  if (rc) return rc;
+  if (!out || out == psi || out->nq != psi->nq || out->dtype != psi->dtype || out->device != psi->device)
+    return fail(VQC_ERR_ARG, "apply: output must be a distinct state of the same size, dtype and device");
+  std::lock_guard<std::mutex> lk(psi->mu);
+  if ((rc = stream_after(psi, out))) return rc;
+  if ((rc = pauli_run(psi, nullptr, psi->d, out->d, terms, nterms, true, false, false, nullptr))) return rc;
+  return stream_after(out, psi);
+}
+
+int vqc_expect_dense(vqc_state phi, vqc_state psi, int k, const int* pos, const double* mat, double* out) {
+  int rc = enter(psi);
+  if (rc) return rc;
+  if (!out) return fail(VQC_ERR_ARG, "null output");
+  if (phi && (phi->nq != psi->nq || phi->dtype != psi->dtype || phi->device != psi->device))
+    return fail(VQC_ERR_ARG, "expectation: states differ in size, dtype or device");
+  std::lock_guard<std::mutex> lk(psi->mu);
+  int sp[5];
+  std::vector<cd> M;
+  if ((rc = order_matrix(psi->nq, k, pos, mat, sp, M))) return rc;
+  if (phi && (rc = stream_after(psi, phi))) return rc;
+  if ((rc = expect_dense_device(psi, phi ? phi->d : psi->d, psi->d, k, sp, M, psi->scr.result))) return rc;
+  if ((rc = fetch_result(psi, 2))) return rc;
+  out[0] = psi->h_result[0];
+  out[1] = psi->h_result[1];
+  return VQC_OK;
+}
+
+int vqc_apply_dense_add(vqc_state psi, vqc_state out, int k, const int* pos, const double* mat) {
+  int rc = enter(psi);
+  if (rc) return rc;
+  if (!out || out == psi || out->nq != psi->nq || out->dtype != psi->dtype || out->device != psi->device)
+    return fail(VQC_ERR_ARG, "apply: output must be a distinct state of the same size, dtype and device");
+  std::lock_guard<std::mutex> lk(psi->mu);
+  int sp[5];
+  std::vector<cd> M;
+  if ((rc = order_matrix(psi->nq, k, pos, mat, sp, M))) return rc;
+  if ((rc = stream_after(psi, out))) return rc;
+  switch (k) {
+    case 1: rc = apply_dense_ms<2>(psi, psi->d, out->d, k, sp, M); break;
+    case 2: rc = apply_dense_ms<4>(psi, psi->d, out->d, k, sp, M); break;
+    case 3: rc = apply_dense_ms<8>(psi, psi->d, out->d, k, sp, M); break;
+    case 4: rc = apply_dense_ms<16>(psi, psi->d, out->d, k, sp, M); break;
+    default: rc = apply_dense_ms<32>(psi, psi->d, out->d, k, sp, M); break;
+  }
+  if (rc) return rc;
+  return stream_after(out, psi);
+}
+
+}  // extern "C"
