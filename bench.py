@@ -221,9 +221,13 @@ def run_ours(args, rank, world, local_rank):
         grads = np.zeros(packed.nparams)
         energy = (ctypes.c_double * 2)()
         stream = torch.cuda.ExternalStream(lib.vqc_state_stream(psi0.handle), device=local_rank)
+        def upload_host():
+            _lib.check(lib.vqc_state_upload(psi0.handle, ctypes.c_void_p(e2e_host.data_ptr()),
+                                            e2e_host.numel() * e2e_host.element_size()))
+
         for _ in range(warmup):
             if e2e_host is not None:
-                psi0.upload(e2e_host)
+                upload_host()
                 V.energy_and_gradient(H, circuit, psi0)
             else:
                 grad_call(psi0, grads, energy)
@@ -236,9 +240,8 @@ def run_ours(args, rank, world, local_rank):
         start.record(stream)
         for _ in range(steps):
             if e2e_host is not None:
-                _lib.check(lib.vqc_state_upload(psi0.handle, ctypes.c_void_p(e2e_host.data_ptr()),
-                                                e2e_host.numel() * e2e_host.element_size()))
-                e, g = V.energy_and_gradient(H, circuit, psi0)
+                upload_host()
+                V.energy_and_gradient(H, circuit, psi0)
             else:
                 grad_call(psi0, grads, energy)
         end.record(stream)
@@ -269,14 +272,21 @@ def run_ours(args, rank, world, local_rank):
     value = world * 1000.0 / ms
 
     # end to end through the public API with psi0 in pinned host memory
-    host = torch.zeros(2 << N_QUBITS, dtype=torch.float32).pin_memory()
-    host[0] = 1.0
-    ms_e2e, _, _, _ = timed(psi32, max(1, args.steps // 2), 1, e2e_host=host)
+    ms_e2e = None
+    if not args.no_e2e:
+        host = torch.zeros(2 << N_QUBITS, dtype=torch.float32).pin_memory()
+        host[0] = 1.0
+        ms_e2e, _, _, _ = timed(psi32, max(1, args.steps // 2), 1, e2e_host=host)
 
     # the plain FP64 path, for the FP32-vs-FP64 speedup
-    psi64 = make_state(np.complex128)
-    ms64, _, energy64, grads64 = timed(psi64, max(1, args.steps // 2), 1)
-    del psi64
+    fp64 = None
+    if not args.no_fp64:
+        psi64 = make_state(np.complex128)
+        ms64, _, energy64, grads64 = timed(psi64, max(1, args.steps // 2), 1)
+        del psi64
+        fp64 = {"value": world * 1000.0 / ms64, "unit": UNIT, "ms_per_step": ms64, "fp32_speedup": ms64 / ms,
+                "energy_rel_diff_fp32_vs_fp64": abs(energy - energy64) / abs(energy64),
+                "grad_rel_diff_fp32_vs_fp64": float(np.linalg.norm(grads - grads64) / np.linalg.norm(grads64))}
 
     if rank != 0:
         return
@@ -302,12 +312,10 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded angles, |0> input)",
             "config": config_dict(args),
-            "e2e": {"value": world * 1000.0 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": (1 << N_QUBITS) * 8,
-                    "d2h_bytes_per_step": packed.nparams * 8 + 16},
-            "fp64_plain": {"value": world * 1000.0 / ms64, "unit": UNIT, "ms_per_step": ms64,
-                           "fp32_speedup": ms64 / ms,
-                           "energy_rel_diff_fp32_vs_fp64": abs(energy - energy64) / abs(energy64),
-                           "grad_rel_diff_fp32_vs_fp64": float(np.linalg.norm(grads - grads64) / np.linalg.norm(grads64))},
+            "e2e": None if ms_e2e is None else {
+                "value": world * 1000.0 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": (1 << N_QUBITS) * 8,
+                "d2h_bytes_per_step": packed.nparams * 8 + 16},
+            "fp64_plain": fp64,
             "energy": energy.real,
             "roofline": roof, "kernels": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in (prof or {}).items()},
             "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu}
@@ -321,7 +329,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
+    ap.add_argument("--qubits", type=int, default=None,
+                    help="state size (default 26, the headline; smaller sizes are for profiling captures)")
     args = ap.parse_args()
+    if args.qubits is not None:
+        global N_QUBITS
+        N_QUBITS = args.qubits
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
