@@ -122,104 +122,91 @@ static int launch_adj_r(const GateSpec& gd, vqc_state h, void* lam, void* psi, b
   }
 }
 
-struct ParamRef {
-  int index;  // position in the caller's params array
+struct ParamInfo {
+  int index;          // position in the caller's params array
   std::vector<cd> D;  // U^dagger dU/dtheta in sorted order (2^k x 2^k)
 };
+int fused_supported(vqc_state h);
+int reverse_sweep_fused(vqc_state h, void* lam, void* y, const std::vector<GateSpec>& specs,
+                        const std::vector<std::vector<ParamInfo>>& params, double* grads);
+
+// lam, y <- U^dagger (gd holds U^dagger); with acc, out receives A (|S| <= 4).
+int standalone_adjoint(vqc_state h, void* lam, void* y, const GateSpec& gd, bool acc, double* out) {
+  if (gd.ns == 0) return VQC_OK;
+  return h->dtype == VQC_C64 ? launch_adj_r<float>(gd, h, lam, y, acc, out)
+                             : launch_adj_r<double>(gd, h, lam, y, acc, out);
+}
+
+// One gate of the reverse sweep with its parameters' partials, evaluated at
+// once (used for gates the tile engine does not take).
+int per_gate_params_grad(vqc_state h, void* lam, void* y, const GateSpec& gs, const std::vector<ParamInfo>& ps,
+                         double* grads) {
+  const int d = 1 << gs.k;
+  if (gs.ns > 0 && gs.ns <= kAccMaxS) {
+    int rc = standalone_adjoint(h, lam, y, gs, true, h->scr.result);
+    if (rc) return rc;
+    if ((rc = fetch_result(h, 2 * kAccMaxS * kAccMaxS))) return rc;
+    const int MS = ms_of(gs.ns);
+    for (const ParamInfo& pi : ps) {
+      double g = 0;
+      for (int r = 0; r < gs.ns; ++r)
+        for (int c = 0; c < gs.ns; ++c) {
+          const cd Dv = pi.D[(size_t)gs.S[r] * d + gs.S[c]];
+          const cd Av(h->h_result[2 * (r * MS + c)], h->h_result[2 * (r * MS + c) + 1]);
+          g += (Dv * Av).real();
+        }
+      grads[pi.index] = g;
+    }
+    return VQC_OK;
+  }
+  int rc = standalone_adjoint(h, lam, y, gs, false, nullptr);
+  if (rc) return rc;
+  for (const ParamInfo& pi : ps) {
+    if ((rc = expect_dense_device(h, lam, y, gs.k, gs.sp, pi.D, h->scr.result))) return rc;
+    if ((rc = fetch_result(h, 2))) return rc;
+    grads[pi.index] = h->h_result[0];
+  }
+  return VQC_OK;
+}
 
 // The reverse sweep over lam (cotangent) and y (state): both are overwritten
 // with their values at the circuit input; grads[j] receive the partials.
 static int reverse_sweep(vqc_state h, void* lam, void* y, const vqc_gate* gates, int ngates, const double* mats,
-                         const vqc_param* params, int nparams, double* grads) {
+                         const vqc_param* params, int nparams, double* grads, bool fuse) {
   if (nparams < 0 || (nparams > 0 && (!params || !grads))) return fail(VQC_ERR_ARG, "bad parameter arrays");
-  std::vector<std::vector<ParamRef>> per_gate(ngates);
+  std::vector<std::vector<ParamInfo>> per_gate(ngates);
   for (int j = 0; j < nparams; ++j) {
     const int gi = params[j].gate;
     if (gi < 0 || gi >= ngates) return fail(VQC_ERR_ARG, "parameter refers to a gate out of range");
-    per_gate[gi].push_back(ParamRef{j, {}});
+    per_gate[gi].push_back(ParamInfo{j, {}});
   }
-  // device rows for A, one per gate with parameters and |S| <= kAccMaxS
-  int rows = 0;
-  std::vector<int> row_of(ngates, -1);
   std::vector<GateSpec> specs(ngates);
   for (int i = 0; i < ngates; ++i) {
     const vqc_gate& gt = gates[i];
     int rc = analyze_gate(h->nq, gt.nq, gt.pos, mats + gt.mat, true, specs[i]);
     if (rc) return rc;
-    if (!per_gate[i].empty()) {
-      // D_j = U^dagger dU_j, both in sorted order
-      const GateSpec& gs = specs[i];
-      const int d = 1 << gs.k;
-      for (ParamRef& pr : per_gate[i]) {
-        int sp[5];
-        std::vector<cd> dU;
-        if ((rc = order_matrix(h->nq, gt.nq, gt.pos, mats + params[pr.index].dmat, sp, dU))) return rc;
-        pr.D.assign((size_t)d * d, cd(0));
-        for (int r = 0; r < d; ++r)
-          for (int c = 0; c < d; ++c) {
-            cd acc = 0;
-            for (int m = 0; m < d; ++m) acc += gs.U[(size_t)r * d + m] * dU[(size_t)m * d + c];  // gs.U = U^dagger
-            pr.D[(size_t)r * d + c] = acc;
-          }
-      }
-      if (specs[i].ns <= kAccMaxS) row_of[i] = rows++;
-    }
-  }
-  if ((size_t)rows > h->accbuf_rows) {
-    if (h->accbuf) {
-      VQC_CK(cudaStreamSynchronize(h->stream));
-      VQC_CK(cudaFree(h->accbuf));
-      h->accbuf = nullptr;
-    }
-    VQC_CK(cudaMalloc(&h->accbuf, sizeof(double) * 2 * kAccMaxS * kAccMaxS * std::max(rows, 1)));
-    h->accbuf_rows = std::max(rows, 1);
-  }
-  // gates with |S| > kAccMaxS and parameters: one two-state pass per parameter
-  for (int i = ngates - 1; i >= 0; --i) {
     const GateSpec& gs = specs[i];
-    const bool acc = row_of[i] >= 0;
-    double* out = acc ? h->accbuf + (size_t)row_of[i] * 2 * kAccMaxS * kAccMaxS : nullptr;
-    int rc = VQC_OK;
-    if (gs.ns > 0)
-      rc = h->dtype == VQC_C64 ? launch_adj_r<float>(gs, h, lam, y, acc, out)
-                               : launch_adj_r<double>(gs, h, lam, y, acc, out);
-    else if (acc) {
-      // identity gate (e.g. a rotation by 0): A over an empty subspace is unusable,
-      // fall back to direct passes below
-      row_of[i] = -1;
+    const int d = 1 << gs.k;
+    for (ParamInfo& pi : per_gate[i]) {  // D_j = U^dagger dU_j (gs.U holds U^dagger)
+      int sp[5];
+      std::vector<cd> dU;
+      if ((rc = order_matrix(h->nq, gt.nq, gt.pos, mats + params[pi.index].dmat, sp, dU))) return rc;
+      pi.D.assign((size_t)d * d, cd(0));
+      for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) {
+          cd acc = 0;
+          for (int m = 0; m < d; ++m) acc += gs.U[(size_t)r * d + m] * dU[(size_t)m * d + c];
+          pi.D[(size_t)r * d + c] = acc;
+        }
     }
+  }
+  if (fuse && fused_supported(h)) return reverse_sweep_fused(h, lam, y, specs, per_gate, grads);
+  for (int i = ngates - 1; i >= 0; --i) {
+    int rc = per_gate[i].empty() ? standalone_adjoint(h, lam, y, specs[i], false, nullptr)
+                                 : per_gate_params_grad(h, lam, y, specs[i], per_gate[i], grads);
     if (rc) return rc;
-    if (!per_gate[i].empty() && row_of[i] < 0) {
-      for (const ParamRef& pr : per_gate[i]) {
-        if ((rc = expect_dense_device(h, lam, y, gs.k, gs.sp, pr.D, h->scr.result))) return rc;
-        if ((rc = fetch_result(h, 2))) return rc;
-        grads[pr.index] = h->h_result[0];
-      }
-    }
   }
-  if (rows > 0) {
-    std::vector<double> A((size_t)rows * 2 * kAccMaxS * kAccMaxS);
-    VQC_CK(cudaMemcpyAsync(A.data(), h->accbuf, sizeof(double) * A.size(), cudaMemcpyDeviceToHost, h->stream));
-    VQC_CK(cudaStreamSynchronize(h->stream));
-    for (int i = 0; i < ngates; ++i) {
-      if (row_of[i] < 0) continue;
-      const GateSpec& gs = specs[i];
-      const int d = 1 << gs.k, MS = ms_of(gs.ns);
-      const double* a = &A[(size_t)row_of[i] * 2 * kAccMaxS * kAccMaxS];
-      for (const ParamRef& pr : per_gate[i]) {
-        double g = 0;
-        for (int r = 0; r < gs.ns; ++r)
-          for (int c = 0; c < gs.ns; ++c) {
-            const cd Dv = pr.D[(size_t)gs.S[r] * d + gs.S[c]];
-            const cd Av(a[2 * (r * MS + c)], a[2 * (r * MS + c) + 1]);
-            g += (Dv * Av).real();
-          }
-        grads[pr.index] = g;
-      }
-    }
-  } else {
-    VQC_CK(cudaStreamSynchronize(h->stream));
-  }
+  VQC_CK(cudaStreamSynchronize(h->stream));
   return VQC_OK;
 }
 
@@ -250,7 +237,7 @@ int vqc_adjoint_grad(vqc_state psi0, const vqc_gate* gates, int ngates, const do
   if (rc) return rc;
   // E = <y|H|y>; cotangent lam = (conj(z) H + z H^dagger) y with z = 1
   if ((rc = pauli_run(psi0, y, y, lam, terms, nterms, true, true, true, energy))) return rc;
-  return reverse_sweep(psi0, lam, y, gates, ngates, mats, params, nparams, grads);
+  return reverse_sweep(psi0, lam, y, gates, ngates, mats, params, nparams, grads, true);
 }
 
 int vqc_circuit_backward(vqc_state y, vqc_state delta, const vqc_gate* gates, int ngates, const double* mats,
@@ -263,7 +250,7 @@ int vqc_circuit_backward(vqc_state y, vqc_state delta, const vqc_gate* gates, in
   if (ngates < 0 || (ngates > 0 && (!gates || !mats))) return fail(VQC_ERR_ARG, "bad circuit arrays");
   std::lock_guard<std::mutex> lk(y->mu);
   if ((rc = stream_after(y, delta))) return rc;
-  if ((rc = reverse_sweep(y, delta->d, y->d, gates, ngates, mats, params, nparams, grads))) return rc;
+  if ((rc = reverse_sweep(y, delta->d, y->d, gates, ngates, mats, params, nparams, grads, true))) return rc;
   return stream_after(delta, y);
 }
 

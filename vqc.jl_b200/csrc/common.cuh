@@ -118,6 +118,8 @@ struct vqc_state_s {
   void* work[3] = {nullptr, nullptr, nullptr};  // state-sized workspaces (gradients)
   double* accbuf = nullptr;    // gradient partial sums, one row per parameterised gate
   size_t accbuf_rows = 0;
+  void* fused_scratch = nullptr;  // per-CTA partial sums of the tile engine
+  size_t fused_scratch_bytes = 0;
   std::mutex mu;
   size_t amp_bytes() const { return dtype == VQC_C64 ? 8 : 16; }
   int64_t size() const { return int64_t(1) << nq; }

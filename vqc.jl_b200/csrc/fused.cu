@@ -1,15 +1,1085 @@
-// apply!(::QCircuit, state) with gate fusion: placeholder that applies the
-// gates one by one until the tile engine lands.
+// The fused tile engine: apply!(::QCircuit, state) (generic.jl:26-31) and the
+// reverse sweep of the circuit pullback (circuitdiff.jl:61-75) with many gates
+// per HBM round trip.
+//
+// The reference runs one full pass over the state per gate.  Here a host
+// planner groups the gates into *passes*.  A pass picks a set Q of M "tile"
+// qubits (always including the lowest qubits, so every tile is made of
+// contiguous runs of amplitudes); every CTA loads whole tiles (the 2^M
+// amplitudes that share all non-tile bits) into shared memory, applies every
+// gate of the pass to them, and writes them back: one HBM read + write per
+// pass instead of per gate.
+//   * a gate whose matrix acts on one or two target qubits (after stripping
+//     control qubits, read off the matrix) is applied in registers: each
+//     thread holds 16 amplitudes spanning 4 tile bits ("register bits"), and
+//     the pass is cut into *stages*, each with one register-bit set;
+//     between stages the tile goes through shared memory (XOR-swizzled, so
+//     the 16-byte / 8-byte accesses are free of bank conflicts);
+//   * controls on tile bits are tested per amplitude, controls on non-tile
+//     qubits once per tile;
+//   * diagonal gates (CZ, CPHASE, ...) act on any qubits, tile or not;
+//   * consecutive one-qubit gates on the same qubit are merged into one 2x2.
+// In the reverse sweep (ADJ) each op applies U^dagger to both the cotangent
+// and the state and accumulates the reduced matrix
+//   A[a][b] = sum conj(lambda_a) psi_b   over the op's target pairs
+// (per thread over its 8 pairs in the state's precision, then in FP64 across
+// the warp, the CTA and the grid, in a fixed order); the host contracts A
+// with D_j = B^dagger dB/dtheta_j of each parameter j of the (merged) block.
+#include <algorithm>
+#include <cstring>
+#include <map>
+
 #include "engine.h"
+#include "subspace.cuh"
 
 namespace vqc {
 
-int apply_circuit_fused(vqc_state h, const vqc_gate* gates, int ngates, const double* mats) {
-  for (int i = 0; i < ngates; ++i) {
-    int rc = apply_gate_raw(h, gates[i].nq, gates[i].pos, mats + gates[i].mat);
-    if (rc) return rc;
+constexpr int kRegBits = 4;  // 16 amplitudes per thread
+constexpr int kMaxSlots = 64;
+enum { kOpU1 = 1, kOpU2 = 2, kOpDiag = 3, kOpAccD = 4 };
+
+struct DevPass {
+  int64_t dep_hi[16];     // global offset of the 4 top tile bits, per register index
+  uint64_t nontile_mask;  // global bits enumerated by the tile counter
+  uint64_t lo_qmask;      // global qubits of tile bits 0..M-5 (the thread bits at load time)
+  int64_t ntiles;
+  int32_t stage_begin, stage_end;
+  int32_t nslots, pad;
+};
+
+struct DevStage {
+  uint32_t dep[16];   // tile index of register slot j (OR with the thread part)
+  uint32_t thr_mask;  // tile bits held by the thread index, ascending
+  int32_t op_begin, op_end, pad;
+};
+
+struct DevOp {
+  int32_t type;
+  int32_t r0, r1;  // register slots of the targets (U1: r0; U2: r0 < r1, matrix bit 0 <-> r0)
+  int32_t slot;    // accumulation slot or -1
+  uint32_t cmask, cval;  // controls on tile bits
+  uint64_t gmask, gval;  // controls on non-tile qubits
+  int32_t mat;     // pool offset (complex elements)
+  int32_t nd;      // diagonal ops: number of qubits
+  int32_t dbit[5];  // tile bit of diagonal qubit i, or -1
+  int32_t dglob[5]; // global qubit of diagonal qubit i when not a tile bit
+};
+
+// ----------------------------------------------------------------------------- device helpers
+template <class R>
+struct Swz;
+template <>
+struct Swz<float> {  // 8-byte amplitudes: half-warps must hit 16 distinct 8-byte bank pairs
+  __device__ static __forceinline__ uint32_t f(uint32_t t) { return t ^ ((t >> 4) & 15u); }
+};
+template <>
+struct Swz<double> {  // 16-byte amplitudes: quarter-warps must hit 8 distinct 16-byte bank quads
+  __device__ static __forceinline__ uint32_t f(uint32_t t) { return t ^ (((t >> 3) ^ (t >> 6)) & 7u); }
+};
+
+__device__ __forceinline__ int64_t dep64(int64_t v, uint64_t mask) {
+  int64_t r = 0;
+  while (mask) {
+    const uint64_t low = mask & (~mask + 1);
+    if (v & 1) r |= (int64_t)low;
+    v >>= 1;
+    mask ^= low;
+  }
+  return r;
+}
+__device__ __forceinline__ uint32_t dep32(uint32_t v, uint32_t mask) {
+  uint32_t r = 0;
+  while (mask) {
+    const uint32_t low = mask & (~mask + 1);
+    if (v & 1) r |= low;
+    v >>= 1;
+    mask ^= low;
+  }
+  return r;
+}
+
+template <class C>
+__device__ __forceinline__ C ldpool(const C* p) {
+  return __ldg(p);
+}
+
+template <class R>
+__device__ __forceinline__ void acc_pair(R (&a)[8], cplx<R> l0, cplx<R> l1, cplx<R> p0, cplx<R> p1) {
+  // A00 += conj(l0) p0, A01 += conj(l0) p1, A10 += conj(l1) p0, A11 += conj(l1) p1
+  a[0] = fma(l0.x, p0.x, fma(l0.y, p0.y, a[0]));
+  a[1] = fma(l0.x, p0.y, fma(-l0.y, p0.x, a[1]));
+  a[2] = fma(l0.x, p1.x, fma(l0.y, p1.y, a[2]));
+  a[3] = fma(l0.x, p1.y, fma(-l0.y, p1.x, a[3]));
+  a[4] = fma(l1.x, p0.x, fma(l1.y, p0.y, a[4]));
+  a[5] = fma(l1.x, p0.y, fma(-l1.y, p0.x, a[5]));
+  a[6] = fma(l1.x, p1.x, fma(l1.y, p1.y, a[6]));
+  a[7] = fma(l1.x, p1.y, fma(-l1.y, p1.x, a[7]));
+}
+
+// Warp reduce-scatter of 8 values (FP64): afterwards lane L with L % 4 == 0
+// holds the warp total of value L / 4.
+__device__ __forceinline__ double warp_reduce8(const double (&x)[8]) {
+  const int lane = threadIdx.x & 31;
+  double y[4], z[2];
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double keep = b4 ? x[i + 4] : x[i], send = b4 ? x[i] : x[i + 4];
+    y[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double keep = b3 ? y[i + 2] : y[i], send = b3 ? y[i] : y[i + 2];
+    z[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  double u = (b2 ? z[1] : z[0]) + __shfl_xor_sync(0xffffffffu, b2 ? z[0] : z[1], 4);
+  u += __shfl_xor_sync(0xffffffffu, u, 2);
+  u += __shfl_xor_sync(0xffffffffu, u, 1);
+  return u;
+}
+
+template <class R>
+__device__ __forceinline__ void flush_acc(const R (&a)[8], double* sacc, int slot, int nwarps) {
+  double x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x[i] = (double)a[i];
+  const double u = warp_reduce8(x);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if ((lane & 3) == 0) sacc[((size_t)slot * nwarps + warp) * 8 + (lane >> 2)] += u;
+}
+
+// one-qubit op on register slot RR, both states in ADJ mode
+template <int RR, bool ADJ, class R>
+__device__ __forceinline__ void op_u1(cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm, uint32_t cv,
+                                      uint32_t tthr, const uint32_t (&dep)[16], bool acc, double* sacc, int slot,
+                                      int nwarps) {
+  const cplx<R> u00 = ldpool(U), u01 = ldpool(U + 1), u10 = ldpool(U + 2), u11 = ldpool(U + 3);
+  R a[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) a[i] = R(0);
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    const int j0 = ((p >> RR) << (RR + 1)) | (p & ((1 << RR) - 1)), j1 = j0 | (1 << RR);
+    if (((tthr | dep[j0]) & cm) == cv) {
+      const cplx<R> x0 = v[j0], x1 = v[j1];
+      v[j0] = cfma(u01, x1, cmul(u00, x0));
+      v[j1] = cfma(u11, x1, cmul(u10, x0));
+      if (ADJ) {
+        const cplx<R> y0 = w[j0], y1 = w[j1];
+        w[j0] = cfma(u01, y1, cmul(u00, y0));
+        w[j1] = cfma(u11, y1, cmul(u10, y0));
+        if (acc) acc_pair<R>(a, w[j0], w[j1], v[j0], v[j1]);
+      }
+    }
+  }
+  if (ADJ && acc) flush_acc<R>(a, sacc, slot, nwarps);
+}
+
+// two-qubit op on register slots (RA < RB), matrix bit 0 <-> RA
+template <int RA, int RB, bool ADJ, class R>
+__device__ __forceinline__ void op_u2(cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm, uint32_t cv,
+                                      uint32_t tthr, const uint32_t (&dep)[16]) {
+  cplx<R> m[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) m[i] = ldpool(U + i);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    // insert zero bits at RA and RB into the 2-bit counter q
+    int j = q;
+    j = ((j >> RA) << (RA + 1)) | (j & ((1 << RA) - 1));
+    j = ((j >> RB) << (RB + 1)) | (j & ((1 << RB) - 1));
+    const int i0 = j, i1 = j | (1 << RA), i2 = j | (1 << RB), i3 = j | (1 << RA) | (1 << RB);
+    if (((tthr | dep[i0]) & cm) == cv) {
+      cplx<R> x[4] = {v[i0], v[i1], v[i2], v[i3]};
+      cplx<R> o[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        o[r] = cmul(m[4 * r], x[0]);
+#pragma unroll
+        for (int c = 1; c < 4; ++c) o[r] = cfma(m[4 * r + c], x[c], o[r]);
+      }
+      v[i0] = o[0];
+      v[i1] = o[1];
+      v[i2] = o[2];
+      v[i3] = o[3];
+      if (ADJ) {
+        cplx<R> y[4] = {w[i0], w[i1], w[i2], w[i3]};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          o[r] = cmul(m[4 * r], y[0]);
+#pragma unroll
+          for (int c = 1; c < 4; ++c) o[r] = cfma(m[4 * r + c], y[c], o[r]);
+        }
+        w[i0] = o[0];
+        w[i1] = o[1];
+        w[i2] = o[2];
+        w[i3] = o[3];
+      }
+    }
+  }
+}
+
+template <bool ADJ, class R>
+__device__ __forceinline__ void dispatch_u1(int r, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm,
+                                            uint32_t cv, uint32_t tthr, const uint32_t (&dep)[16], bool acc,
+                                            double* sacc, int slot, int nwarps) {
+  switch (r) {
+    case 0: op_u1<0, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 1: op_u1<1, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 2: op_u1<2, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    default: op_u1<3, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+  }
+}
+
+template <bool ADJ, class R>
+__device__ __forceinline__ void dispatch_u2(int ra, int rb, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U,
+                                            uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t (&dep)[16]) {
+  switch (ra * 4 + rb) {
+    case 1: op_u2<0, 1, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
+    case 2: op_u2<0, 2, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
+    case 3: op_u2<0, 3, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
+    case 6: op_u2<1, 2, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
+    case 7: op_u2<1, 3, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
+    default: op_u2<2, 3, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
+  }
+}
+
+// The tile kernel: one launch per pass, persistent over the tiles.
+template <class R, int M, bool ADJ>
+__global__ void __launch_bounds__(1 << (M - kRegBits), 2)
+    k_tile(cplx<R>* __restrict__ psi, cplx<R>* __restrict__ lam, const DevPass* __restrict__ pass,
+           const DevStage* __restrict__ stages, const DevOp* __restrict__ ops, const cplx<R>* __restrict__ pool,
+           double* __restrict__ partials) {
+  constexpr int NT = 1 << (M - kRegBits), T = 1 << M, NW = NT / 32;
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  C* sp = reinterpret_cast<C*>(smem);
+  C* sl = sp + (ADJ ? T : 0);
+  double* sacc = reinterpret_cast<double*>(smem + (ADJ ? 2 : 1) * T * sizeof(C));
+  __shared__ DevPass P;
+  if (threadIdx.x == 0) P = *pass;
+  __syncthreads();
+  const int nslots = ADJ ? P.nslots : 0;
+  for (int i = threadIdx.x; i < nslots * NW * 8; i += NT) sacc[i] = 0;
+  const int64_t gthr = dep64(threadIdx.x, P.lo_qmask);
+  C v[16], w[16];
+  for (int64_t tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
+    const int64_t base = dep64(tile, P.nontile_mask);
+    // HBM -> shared (coalesced: consecutive threads hold consecutive low tile bits)
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int64_t gi = base + gthr + P.dep_hi[k];
+      v[k] = psi[gi];
+      if (ADJ) w[k] = lam[gi];
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t t = Swz<R>::f(threadIdx.x + k * NT);
+      sp[t] = v[k];
+      if (ADJ) sl[t] = w[k];
+    }
+    __syncthreads();
+    for (int s = P.stage_begin; s < P.stage_end; ++s) {
+      const DevStage* S = stages + s;
+      uint32_t dep[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) dep[j] = __ldg(&S->dep[j]);
+      const uint32_t tthr = dep32(threadIdx.x, __ldg(&S->thr_mask));
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const uint32_t t = Swz<R>::f(tthr | dep[j]);
+        v[j] = sp[t];
+        if (ADJ) w[j] = sl[t];
+      }
+      const int ob = __ldg(&S->op_begin), oe = __ldg(&S->op_end);
+      for (int o = ob; o < oe; ++o) {
+        const DevOp* op = ops + o;
+        const int type = __ldg(&op->type);
+        const uint64_t gm = __ldg(&op->gmask);
+        if ((base & (int64_t)gm) != (int64_t)__ldg(&op->gval)) continue;  // a non-tile control is off
+        const uint32_t cm = __ldg(&op->cmask), cv = __ldg(&op->cval);
+        const C* U = pool + __ldg(&op->mat);
+        if (type == kOpU1) {
+          const int slot = __ldg(&op->slot);
+          dispatch_u1<ADJ, R>(__ldg(&op->r0), v, w, U, cm, cv, tthr, dep, ADJ && slot >= 0, sacc, slot, NW);
+        } else if (type == kOpU2) {
+          dispatch_u2<ADJ, R>(__ldg(&op->r0), __ldg(&op->r1), v, w, U, cm, cv, tthr, dep);
+        } else {
+          // diagonal: phase index from the op's qubits (tile bits per amplitude, others per tile)
+          const int nd = __ldg(&op->nd);
+          uint32_t gidx = 0;
+          int db[5];
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            db[i] = i < nd ? __ldg(&op->dbit[i]) : -1;
+            if (i < nd && db[i] < 0) gidx |= (uint32_t)((base >> __ldg(&op->dglob[i])) & 1) << i;
+          }
+          if (type == kOpDiag) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const uint32_t t = tthr | dep[j];
+              uint32_t idx = gidx;
+#pragma unroll
+              for (int i = 0; i < 5; ++i)
+                if (db[i] >= 0) idx |= ((t >> db[i]) & 1u) << i;
+              const C d = ldpool(U + idx);
+              v[j] = cmul(d, v[j]);
+              if (ADJ) w[j] = cmul(d, w[j]);
+            }
+          } else if (ADJ) {
+            // kOpAccD: bins of conj(lam) psi over the op's (at most 2) qubits
+            R a[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = R(0);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const uint32_t t = tthr | dep[j];
+              uint32_t idx = gidx;
+#pragma unroll
+              for (int i = 0; i < 2; ++i)
+                if (db[i] >= 0) idx |= ((t >> db[i]) & 1u) << i;
+              const C l = w[j], p = v[j];
+              const R re = fma(l.x, p.x, l.y * p.y), im = fma(l.x, p.y, -l.y * p.x);
+#pragma unroll
+              for (int b = 0; b < 4; ++b)
+                if (idx == (uint32_t)b) {
+                  a[2 * b] += re;
+                  a[2 * b + 1] += im;
+                }
+            }
+            flush_acc<R>(a, sacc, __ldg(&op->slot), NW);
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const uint32_t t = Swz<R>::f(tthr | dep[j]);
+        sp[t] = v[j];
+        if (ADJ) sl[t] = w[j];
+      }
+      __syncthreads();
+    }
+    // shared -> HBM
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t t = Swz<R>::f(threadIdx.x + k * NT);
+      v[k] = sp[t];
+      if (ADJ) w[k] = sl[t];
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int64_t gi = base + gthr + P.dep_hi[k];
+      psi[gi] = v[k];
+      if (ADJ) lam[gi] = w[k];
+    }
+    __syncthreads();
+  }
+  if (ADJ && nslots > 0) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < nslots * 8; i += NT) {
+      const int slot = i >> 3, val = i & 7;
+      double s = 0;
+      for (int wp = 0; wp < NW; ++wp) s += sacc[((size_t)slot * NW + wp) * 8 + val];
+      partials[((size_t)blockIdx.x * nslots + slot) * 8 + val] = s;
+    }
+  }
+}
+
+// Sums the per-CTA partials over the grid in a fixed order: block = slot.
+__global__ void __launch_bounds__(256) k_reduce_slots(const double* __restrict__ partials, int nblocks, int nslots,
+                                                      int row0, double* __restrict__ out) {
+  __shared__ double sm[8][8];
+  const int slot = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int val = 0; val < 8; ++val) {
+    double s = 0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[((size_t)b * nslots + slot) * 8 + val];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) sm[warp][val] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    double s = 0;
+    for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) s += sm[wp][threadIdx.x];
+    out[(size_t)(row0 + slot) * 8 + threadIdx.x] = s;
+  }
+}
+
+// ----------------------------------------------------------------------------- host planner
+struct PGrad {
+  int param;             // caller's parameter index
+  std::vector<cd> D;     // U1: 2x2 over the target (control subspace); AccD: 2^nd diagonal bins
+};
+
+struct FOp {
+  int kind = 0;          // kOpU1, kOpU2, kOpDiag, kOpAccD
+  int tq[2] = {-1, -1};  // target qubits (ascending)
+  uint64_t cmask = 0, cval = 0;  // control qubits and their firing values (global bits)
+  uint64_t qubits = 0;   // every qubit the op reads or writes
+  std::vector<cd> mat;   // U1 2x2, U2 4x4 (bit 0 <-> tq[0]), diagonal 2^nd table
+  int nd = 0;
+  int dq[5] = {0, 0, 0, 0, 0};
+  bool acc = false;
+  std::vector<PGrad> grads;
+};
+
+// A gate in planner form: one op, or "standalone" (kept as a GateSpec).
+struct PItem {
+  bool standalone = false;
+  int gate = -1;  // index in the caller's gate list
+  FOp op;
+};
+
+static inline int popc64(uint64_t x) { return __builtin_popcountll(x); }
+
+// Reads a gate's structure off its (sorted, possibly daggered) matrix.
+// Returns false when the gate cannot be fused (3+ target qubits).
+static bool to_fop(const GateSpec& g, FOp& f) {
+  const int k = g.k, d = 1 << k;
+  f = FOp();
+  for (int b = 0; b < k; ++b) f.qubits |= 1ull << g.sp[b];
+  if (g.ns == 0) {  // identity
+    f.kind = kOpDiag;
+    f.nd = 0;
+    f.mat = {cd(1)};
+    return true;
+  }
+  if (k == 1) {  // one-qubit gates (diagonal ones too) run in registers and merge
+    f.kind = kOpU1;
+    f.tq[0] = g.sp[0];
+    f.mat = g.U;
+    return true;
+  }
+  if (g.mode == kDiag) {
+    f.kind = kOpDiag;
+    f.nd = k;
+    for (int b = 0; b < k; ++b) f.dq[b] = g.sp[b];
+    f.mat.resize(d);
+    for (int j = 0; j < d; ++j) f.mat[j] = g.U[(size_t)j * d + j];
+    return true;
+  }
+  // controls: bits constant over the active set
+  int ctrl_bits = 0, cval_bits = 0;
+  for (int b = 0; b < k; ++b) {
+    bool all1 = true, all0 = true;
+    for (int s = 0; s < g.ns; ++s) {
+      if (g.S[s] >> b & 1)
+        all0 = false;
+      else
+        all1 = false;
+    }
+    if (all1 || all0) {
+      ctrl_bits |= 1 << b;
+      if (all1) cval_bits |= 1 << b;
+    }
+  }
+  int tb[5], nt = 0;
+  for (int b = 0; b < k; ++b)
+    if (!(ctrl_bits >> b & 1)) tb[nt++] = b;
+  if (nt == 0 || nt > 2) return false;
+  for (int b = 0; b < k; ++b)
+    if (ctrl_bits >> b & 1) {
+      f.cmask |= 1ull << g.sp[b];
+      if (cval_bits >> b & 1) f.cval |= 1ull << g.sp[b];
+    }
+  f.kind = nt == 1 ? kOpU1 : kOpU2;
+  for (int i = 0; i < nt; ++i) f.tq[i] = g.sp[tb[i]];
+  const int dn = 1 << nt;
+  f.mat.assign((size_t)dn * dn, cd(0));
+  auto full = [&](int a) {  // target-subspace index -> gate index
+    int j = cval_bits;
+    for (int i = 0; i < nt; ++i)
+      if (a >> i & 1) j |= 1 << tb[i];
+    return j;
+  };
+  for (int a = 0; a < dn; ++a)
+    for (int c = 0; c < dn; ++c) f.mat[(size_t)a * dn + c] = g.U[(size_t)full(a) * d + full(c)];
+  return true;
+}
+
+// Restriction of a full sorted-order k-qubit matrix to the op's target subspace.
+static std::vector<cd> restrict_to(const GateSpec& g, const FOp& f, const std::vector<cd>& D) {
+  const int k = g.k, d = 1 << k;
+  int cval_bits = 0, tb[2], nt = 0;
+  for (int b = 0; b < k; ++b) {
+    const uint64_t q = 1ull << g.sp[b];
+    if (f.cmask & q) {
+      if (f.cval & q) cval_bits |= 1 << b;
+    } else {
+      tb[nt++] = b;
+    }
+  }
+  const int dn = 1 << nt;
+  std::vector<cd> R((size_t)dn * dn);
+  auto full = [&](int a) {
+    int j = cval_bits;
+    for (int i = 0; i < nt; ++i)
+      if (a >> i & 1) j |= 1 << tb[i];
+    return j;
+  };
+  for (int a = 0; a < dn; ++a)
+    for (int c = 0; c < dn; ++c) R[(size_t)a * dn + c] = D[(size_t)full(a) * d + full(c)];
+  return R;
+}
+
+static void mat2_mul(const std::vector<cd>& A, const std::vector<cd>& B, std::vector<cd>& C) {  // C = A B
+  C.assign(4, cd(0));
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 2; ++c) C[r * 2 + c] = A[r * 2] * B[c] + A[r * 2 + 1] * B[2 + c];
+}
+static std::vector<cd> mat2_dag(const std::vector<cd>& A) {
+  return {std::conj(A[0]), std::conj(A[2]), std::conj(A[1]), std::conj(A[3])};
+}
+
+struct PlanStage {
+  std::vector<int> rs;   // tile-bit indices (ascending)
+  std::vector<int> ops;  // indices into PlanPass::ops
+};
+struct PlanPass {
+  bool standalone = false;
+  int gate = -1;                 // standalone: the caller's gate
+  std::vector<int> tile_q;       // M global qubits, ascending
+  std::vector<FOp> ops;
+  std::vector<PlanStage> stages;
+  int nslots = 0;
+};
+
+struct TileConfig {
+  int M;      // tile bits
+  int clow;   // always-resident low qubits
+};
+
+static TileConfig tile_config(int dtype, bool adj) {
+  (void)adj;
+  if (dtype == VQC_C64) return {12, 4};
+  return {11, 3};
+}
+
+// Greedy pass formation (see the file comment).  items are in execution order.
+static void plan_passes(int n, const TileConfig& tc, bool adj, std::vector<PItem>& items, std::vector<PlanPass>& out) {
+  const int M = tc.M;
+  std::vector<char> done(items.size(), 0);
+  size_t first = 0;
+  while (true) {
+    while (first < items.size() && done[first]) ++first;
+    if (first >= items.size()) break;
+    if (items[first].standalone) {
+      PlanPass p;
+      p.standalone = true;
+      p.gate = items[first].gate;
+      out.push_back(std::move(p));
+      done[first] = 1;
+      continue;
+    }
+    PlanPass p;
+    uint64_t Q = 0;
+    for (int q = 0; q < std::min(tc.clow, n); ++q) Q |= 1ull << q;
+    uint64_t blocked = 0;
+    std::vector<int> last_on(n, -1);  // last op index in p.ops touching qubit q
+    for (size_t i = first; i < items.size(); ++i) {
+      if (done[i]) continue;
+      PItem& it = items[i];
+      const uint64_t qs = it.op.qubits;
+      if (it.standalone) {  // runs after this pass: its qubits stay blocked
+        blocked |= qs;
+        continue;
+      }
+      if (qs & blocked) {
+        blocked |= qs;
+        continue;
+      }
+      FOp& f = it.op;
+      uint64_t need = 0;
+      if (f.kind == kOpU1) need = 1ull << f.tq[0];
+      if (f.kind == kOpU2) need = (1ull << f.tq[0]) | (1ull << f.tq[1]);
+      const bool fits = popc64(Q | need) <= M;
+      const bool slot_ok = !(adj && f.acc) || p.nslots < kMaxSlots;
+      if (!fits || !slot_ok) {
+        blocked |= qs;
+        continue;
+      }
+      Q |= need;
+      done[i] = 1;
+      // merge consecutive uncontrolled one-qubit ops on the same qubit
+      if (f.kind == kOpU1 && f.cmask == 0) {
+        const int prev = last_on[f.tq[0]];
+        if (prev >= 0) {
+          FOp& g = p.ops[prev];
+          if (g.kind == kOpU1 && g.cmask == 0 && g.tq[0] == f.tq[0]) {
+            // g applied first, then f: merged = f.mat * g.mat
+            std::vector<cd> merged;
+            mat2_mul(f.mat, g.mat, merged);
+            if (adj) {
+              // g's gradients were taken at g's output side = f's input: move them
+              // to the block input (f is applied after g, so D -> F^dag D F)
+              const std::vector<cd> Fd = mat2_dag(f.mat);
+              for (PGrad& pg : g.grads) {
+                std::vector<cd> t1, t2;
+                // in the reverse sweep the op matrices are U^dagger: f.mat = U_f^dagger,
+                // the block input lies after f, and D_g moves by conjugation with f.mat^dagger
+                mat2_mul(pg.D, Fd, t1);
+                mat2_mul(f.mat, t1, t2);
+                pg.D = t2;
+              }
+              for (PGrad& pg : f.grads) g.grads.push_back(pg);
+              if (f.acc && !g.acc) {
+                g.acc = true;
+                ++p.nslots;
+              }
+            }
+            g.mat = merged;
+            continue;
+          }
+        }
+      }
+      if (adj && f.acc) ++p.nslots;
+      p.ops.push_back(f);
+      for (int q = 0; q < n; ++q)
+        if (qs >> q & 1) last_on[q] = (int)p.ops.size() - 1;
+    }
+    // fill the tile with the lowest remaining qubits
+    for (int q = 0; q < n && popc64(Q) < M; ++q) Q |= 1ull << q;
+    for (int q = 0; q < n; ++q)
+      if (Q >> q & 1) p.tile_q.push_back(q);
+    out.push_back(std::move(p));
+  }
+}
+
+// Conflict check of a register-bit set for the shared-memory swizzle.
+static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype) {
+  std::vector<int> lanes;
+  for (int b = 0; b < M && (int)lanes.size() < (dtype == VQC_C64 ? 4 : 3); ++b)
+    if (std::find(rs.begin(), rs.end(), b) == rs.end()) lanes.push_back(b);
+  int seen = 0;
+  for (int b : lanes) {
+    int res;
+    if (dtype == VQC_C64)
+      res = b < 4 ? b : (b < 8 ? b - 4 : -1);
+    else
+      res = b < 3 ? b : (b < 9 ? (b - 3) % 3 : -1);
+    if (res < 0 || (seen >> res & 1)) return false;
+    seen |= 1 << res;
+  }
+  return true;
+}
+
+static void plan_stages(PlanPass& p, int M, int dtype) {
+  std::map<int, int> tbit;  // global qubit -> tile bit
+  for (int b = 0; b < (int)p.tile_q.size(); ++b) tbit[p.tile_q[b]] = b;
+  std::vector<int> pending(p.ops.size());
+  for (size_t i = 0; i < pending.size(); ++i) pending[i] = (int)i;
+  while (!pending.empty()) {
+    PlanStage st;
+    uint64_t blocked = 0;
+    std::vector<int> rest;
+    std::vector<int> rs;
+    for (int oi : pending) {
+      const FOp& f = p.ops[oi];
+      if (f.qubits & blocked) {
+        blocked |= f.qubits;
+        rest.push_back(oi);
+        continue;
+      }
+      std::vector<int> need;
+      if (f.kind == kOpU1) need = {tbit[f.tq[0]]};
+      if (f.kind == kOpU2) need = {tbit[f.tq[0]], tbit[f.tq[1]]};
+      std::vector<int> u = rs;
+      for (int b : need)
+        if (std::find(u.begin(), u.end(), b) == u.end()) u.push_back(b);
+      if ((int)u.size() <= kRegBits) {
+        rs = u;
+        st.ops.push_back(oi);
+      } else {
+        blocked |= f.qubits;
+        rest.push_back(oi);
+      }
+    }
+    // fill the register set to 4 bits, preferring a conflict-free layout
+    std::vector<int> cand;
+    for (int b = 0; b < M; ++b)
+      if (std::find(rs.begin(), rs.end(), b) == rs.end()) cand.push_back(b);
+    const int need_more = kRegBits - (int)rs.size();
+    std::vector<int> best;
+    bool found = false;
+    const int nc = std::min((int)cand.size(), 10);
+    for (int mask = 0; mask < (1 << nc) && !found; ++mask) {
+      if (popc64((uint64_t)mask) != need_more) continue;
+      std::vector<int> t = rs;
+      for (int i = 0; i < nc; ++i)
+        if (mask >> i & 1) t.push_back(cand[i]);
+      std::sort(t.begin(), t.end());
+      if (best.empty()) best = t;
+      if (rs_conflict_free(t, M, dtype)) {
+        best = t;
+        found = true;
+      }
+    }
+    st.rs = best;
+    p.stages.push_back(st);
+    pending = rest;
+  }
+}
+
+// ----------------------------------------------------------------------------- execution
+struct Device {
+  std::vector<unsigned char> buf;
+  template <class T>
+  size_t put(const T* p, size_t n) {
+    size_t off = (buf.size() + 15) & ~size_t(15);
+    buf.resize(off + sizeof(T) * n);
+    std::memcpy(buf.data() + off, p, sizeof(T) * n);
+    return off;
+  }
+};
+
+template <class R, int M, bool ADJ>
+static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, const DevStage* ds, const DevOp* dops,
+                       const void* pool, double* partials, int grid, int nslots) {
+  constexpr int NT = 1 << (M - kRegBits), T = 1 << M;
+  const size_t smem = (size_t)(ADJ ? 2 : 1) * T * sizeof(cplx<R>) + (ADJ ? (size_t)nslots * (NT / 32) * 8 * 8 : 0);
+  auto kfun = k_tile<R, M, ADJ>;
+  VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
+  ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward",
+                 (double)(ADJ ? 4 : 2) * h->size() * sizeof(cplx<R>));
+  kfun<<<grid, NT, smem, h->stream>>>((cplx<R>*)psi, (cplx<R>*)lam, dp, ds, dops, (const cplx<R>*)pool, partials);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+template <class R, int M, bool ADJ>
+static int tile_grid(int device, int nslots) {
+  constexpr int NT = 1 << (M - kRegBits), T = 1 << M;
+  const size_t smem = (size_t)(ADJ ? 2 : 1) * T * sizeof(cplx<R>) + (ADJ ? (size_t)nslots * (NT / 32) * 8 * 8 : 0);
+  auto kfun = k_tile<R, M, ADJ>;
+  cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, NT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  return device_info(device).sms * per_sm;
+}
+
+int standalone_adjoint(vqc_state h, void* lam, void* y, const GateSpec& gs, bool acc, double* out);
+
+// Runs a planned sequence of passes.  psi (and lam in ADJ mode) are device
+// buffers of h's size.  specs: the analysed gates (daggered in ADJ mode);
+// rows_out (ADJ): device rows of 8 doubles per accumulation, filled in pass
+// order; returns the list of (row, op) in `accs`.
+struct AccRef {
+  int row;
+  FOp op;
+};
+
+template <class R, int M, bool ADJ>
+static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
+                    std::vector<AccRef>* accs, double* rows_dev) {
+  const int n = h->nq;
+  // serialise every pass into one device buffer
+  Device d;
+  std::vector<cplx<R>> pool;
+  struct Loc {
+    size_t pass, stages, ops;
+    int nslots;
+    int row0;
+  };
+  std::vector<Loc> locs(passes.size());
+  int row = 0;
+  for (size_t pi = 0; pi < passes.size(); ++pi) {
+    PlanPass& p = passes[pi];
+    if (p.standalone) continue;
+    plan_stages(p, M, h->dtype);
+    std::vector<DevStage> ds;
+    std::vector<DevOp> dops;
+    std::map<int, int> tbit;
+    for (int b = 0; b < M; ++b) tbit[p.tile_q[b]] = b;
+    uint64_t tile_mask = 0;
+    for (int q : p.tile_q) tile_mask |= 1ull << q;
+    int slot = 0;
+    for (const PlanStage& st : p.stages) {
+      DevStage s{};
+      uint32_t rsmask = 0;
+      for (int b : st.rs) rsmask |= 1u << b;
+      for (int j = 0; j < 16; ++j) {
+        uint32_t t = 0;
+        for (int i = 0; i < kRegBits; ++i)
+          if (j >> i & 1) t |= 1u << st.rs[i];
+        s.dep[j] = t;
+      }
+      s.thr_mask = ((1u << M) - 1) & ~rsmask;
+      s.op_begin = (int)dops.size();
+      for (int oi : st.ops) {
+        const FOp& f = p.ops[oi];
+        DevOp o{};
+        o.type = f.kind;
+        o.slot = -1;
+        auto slot_of = [&](int b) { return (int)(std::find(st.rs.begin(), st.rs.end(), b) - st.rs.begin()); };
+        if (f.kind == kOpU1) o.r0 = slot_of(tbit[f.tq[0]]);
+        if (f.kind == kOpU2) {
+          o.r0 = slot_of(tbit[f.tq[0]]);
+          o.r1 = slot_of(tbit[f.tq[1]]);
+        }
+        for (int q = 0; q < n; ++q) {
+          if (!(f.cmask >> q & 1)) continue;
+          const bool v = f.cval >> q & 1;
+          if (tile_mask >> q & 1) {
+            o.cmask |= 1u << tbit[q];
+            if (v) o.cval |= 1u << tbit[q];
+          } else {
+            o.gmask |= 1ull << q;
+            if (v) o.gval |= 1ull << q;
+          }
+        }
+        o.mat = (int)pool.size();
+        for (const cd& c : f.mat) pool.push_back(mkc<R>((R)c.real(), (R)c.imag()));
+        o.nd = f.nd;
+        for (int i = 0; i < 5; ++i) {
+          o.dbit[i] = -1;
+          o.dglob[i] = 0;
+          if (i < f.nd) {
+            if (tile_mask >> f.dq[i] & 1)
+              o.dbit[i] = tbit[f.dq[i]];
+            else
+              o.dglob[i] = f.dq[i];
+          }
+        }
+        if (ADJ && f.acc) {
+          o.slot = slot++;
+          if (f.kind == kOpDiag) {
+            // the accumulation runs as its own op right after the diagonal
+            dops.push_back(o);
+            DevOp a = o;
+            a.type = kOpAccD;
+            dops.push_back(a);
+            if (accs) accs->push_back(AccRef{row + o.slot, f});
+            continue;
+          }
+          if (accs) accs->push_back(AccRef{row + o.slot, f});
+        }
+        dops.push_back(o);
+      }
+      s.op_end = (int)dops.size();
+      ds.push_back(s);
+    }
+    p.nslots = slot;
+    DevPass P{};
+    P.nontile_mask = ((n >= 64) ? ~0ull : ((1ull << n) - 1)) & ~tile_mask;
+    P.lo_qmask = 0;
+    for (int b = 0; b < M - kRegBits; ++b) P.lo_qmask |= 1ull << p.tile_q[b];
+    for (int k = 0; k < 16; ++k) {
+      int64_t off = 0;
+      for (int i = 0; i < kRegBits; ++i)
+        if (k >> i & 1) off |= int64_t(1) << p.tile_q[M - kRegBits + i];
+      P.dep_hi[k] = off;
+    }
+    P.ntiles = int64_t(1) << (n - M);
+    P.nslots = slot;
+    locs[pi].row0 = row;
+    row += slot;
+    locs[pi].nslots = slot;
+    // stage indices are local to this pass's stage array
+    P.stage_begin = 0;
+    P.stage_end = (int)ds.size();
+    locs[pi].pass = d.put(&P, 1);
+    locs[pi].stages = d.put(ds.data(), ds.size());
+    // op indices in stages are local to this pass's op array
+    locs[pi].ops = d.put(dops.data(), std::max<size_t>(dops.size(), 1));
+  }
+  const size_t pool_off = d.put(pool.data(), std::max<size_t>(pool.size(), 1));
+  int rc = upload_ops(h, d.buf.data(), d.buf.size());
+  if (rc) return rc;
+  const unsigned char* base = (const unsigned char*)h->opbuf;
+  // partial sums scratch: one row of 8 doubles per (CTA, slot) of the largest pass
+  size_t need = 0;
+  for (size_t pi = 0; pi < passes.size(); ++pi)
+    if (!passes[pi].standalone && locs[pi].nslots > 0)
+      need = std::max(need, (size_t)tile_grid<R, M, ADJ>(h->device, locs[pi].nslots) * locs[pi].nslots * 8 *
+                                sizeof(double));
+  double* partials = nullptr;
+  if (ADJ && need > 0) {
+    if (need > h->fused_scratch_bytes) {
+      if (h->fused_scratch) {
+        VQC_CK(cudaStreamSynchronize(h->stream));
+        VQC_CK(cudaFree(h->fused_scratch));
+        h->fused_scratch = nullptr;
+      }
+      VQC_CK(cudaMalloc(&h->fused_scratch, need));
+      h->fused_scratch_bytes = need;
+    }
+    partials = (double*)h->fused_scratch;
+  }
+  for (size_t pi = 0; pi < passes.size(); ++pi) {
+    PlanPass& p = passes[pi];
+    if (p.standalone) {
+      const GateSpec& gs = specs[p.gate];
+      if (ADJ) {
+        if ((rc = standalone_adjoint(h, lam, psi, gs, false, nullptr))) return rc;
+      } else {
+        if ((rc = launch_gate(gs, psi, n, h->dtype, h->device, h->stream))) return rc;
+      }
+      continue;
+    }
+    const int nslots = locs[pi].nslots;
+    const int grid = tile_grid<R, M, ADJ>(h->device, nslots);
+    if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, (const DevPass*)(base + locs[pi].pass),
+                                      (const DevStage*)(base + locs[pi].stages), (const DevOp*)(base + locs[pi].ops),
+                                      base + pool_off, partials, grid, nslots)))
+      return rc;
+    if (ADJ && nslots > 0) {
+      k_reduce_slots<<<nslots, 256, 0, h->stream>>>(partials, grid, nslots, locs[pi].row0, rows_dev);
+      VQC_CK(cudaGetLastError());
+    }
   }
   return VQC_OK;
+}
+
+int fused_supported(vqc_state h) {
+  const TileConfig tc = tile_config(h->dtype, false);
+  return h->nq >= tc.M && h->nq <= 40;
+}
+
+template <class R, int M>
+static int forward_impl(vqc_state h, const vqc_gate* gates, int ngates, const double* mats) {
+  std::vector<GateSpec> specs(ngates);
+  std::vector<PItem> items(ngates);
+  for (int i = 0; i < ngates; ++i) {
+    int rc = analyze_gate(h->nq, gates[i].nq, gates[i].pos, mats + gates[i].mat, false, specs[i]);
+    if (rc) return rc;
+    items[i].gate = i;
+    items[i].standalone = !to_fop(specs[i], items[i].op);
+  }
+  std::vector<PlanPass> passes;
+  plan_passes(h->nq, tile_config(h->dtype, false), false, items, passes);
+  return run_plan<R, M, false>(h, h->d, nullptr, passes, specs, nullptr, nullptr);
+}
+
+int apply_circuit_fused(vqc_state h, const vqc_gate* gates, int ngates, const double* mats) {
+  if (!fused_supported(h)) {
+    for (int i = 0; i < ngates; ++i) {
+      int rc = apply_gate_raw(h, gates[i].nq, gates[i].pos, mats + gates[i].mat);
+      if (rc) return rc;
+    }
+    return VQC_OK;
+  }
+  return h->dtype == VQC_C64 ? forward_impl<float, 12>(h, gates, ngates, mats)
+                             : forward_impl<double, 11>(h, gates, ngates, mats);
+}
+
+// Reverse sweep on the tile engine.  grads[j] receive the partials.  Gates
+// the tile engine cannot take (3+ targets, or 2 targets with parameters) run
+// through the per-gate adjoint path.
+struct ParamInfo {
+  int index;
+  std::vector<cd> D;  // U^dagger dU/dtheta, sorted order
+};
+int per_gate_params_grad(vqc_state h, void* lam, void* y, const GateSpec& gs, const std::vector<ParamInfo>& ps,
+                         double* grads);
+
+template <class R, int M>
+static int reverse_impl(vqc_state h, void* lam, void* y, const std::vector<GateSpec>& specs,
+                        const std::vector<std::vector<ParamInfo>>& params, double* grads) {
+  const int ng = (int)specs.size();
+  std::vector<PItem> items;
+  items.reserve(ng);
+  for (int i = ng - 1; i >= 0; --i) {
+    PItem it;
+    it.gate = i;
+    const GateSpec& gs = specs[i];
+    bool ok = to_fop(gs, it.op);
+    if (ok && !params[i].empty()) {
+      FOp& f = it.op;
+      if (f.kind == kOpU1) {
+        f.acc = true;
+        for (const ParamInfo& pi : params[i]) f.grads.push_back(PGrad{pi.index, restrict_to(gs, f, pi.D)});
+      } else if (f.kind == kOpDiag && f.nd <= 2 && f.nd >= 1) {
+        f.acc = true;
+        const int d = 1 << gs.k;
+        for (const ParamInfo& pi : params[i]) {
+          PGrad pg{pi.index, {}};
+          for (int j = 0; j < d; ++j) pg.D.push_back(pi.D[(size_t)j * d + j]);
+          f.grads.push_back(pg);
+        }
+      } else {
+        ok = false;
+      }
+    }
+    it.standalone = !ok;
+    items.push_back(std::move(it));
+  }
+  std::vector<PlanPass> passes;
+  plan_passes(h->nq, tile_config(h->dtype, true), true, items, passes);
+  // standalone gates with parameters: split their passes out so the per-gate
+  // path can evaluate the partials right after the uncompute
+  std::vector<AccRef> accs;
+  int total_rows = 0;
+  for (auto& p : passes)
+    if (!p.standalone) {
+      int s = 0;
+      for (auto& f : p.ops) s += f.acc ? 1 : 0;
+      total_rows += s;
+    }
+  if ((size_t)total_rows * 8 > h->accbuf_rows * 32) {
+    if (h->accbuf) {
+      VQC_CK(cudaStreamSynchronize(h->stream));
+      VQC_CK(cudaFree(h->accbuf));
+      h->accbuf = nullptr;
+    }
+    const size_t rows32 = ((size_t)total_rows * 8 + 31) / 32 + 1;
+    VQC_CK(cudaMalloc(&h->accbuf, sizeof(double) * 32 * rows32));
+    h->accbuf_rows = rows32;
+  }
+  // run pass by pass so that standalone gates with parameters see the right states
+  std::vector<PlanPass> one(1);
+  int row_base = 0;
+  for (size_t pi = 0; pi < passes.size(); ++pi) {
+    if (passes[pi].standalone) {
+      const int gi = passes[pi].gate;
+      const GateSpec& gs = specs[gi];
+      if (params[gi].empty()) {
+        int rc = standalone_adjoint(h, lam, y, gs, false, nullptr);
+        if (rc) return rc;
+      } else {
+        int rc = per_gate_params_grad(h, lam, y, gs, params[gi], grads);
+        if (rc) return rc;
+      }
+      continue;
+    }
+    // group consecutive tile passes into one upload
+    size_t pj = pi;
+    std::vector<PlanPass> group;
+    while (pj < passes.size() && !passes[pj].standalone) group.push_back(std::move(passes[pj++]));
+    std::vector<AccRef> gaccs;
+    int rc = run_plan<R, M, true>(h, y, lam, group, specs, &gaccs, h->accbuf + (size_t)row_base * 8);
+    if (rc) return rc;
+    for (auto& a : gaccs) {
+      a.row += row_base;
+      accs.push_back(std::move(a));
+    }
+    for (auto& g : group) row_base += g.nslots;
+    pi = pj - 1;
+  }
+  // contract A with the D matrices
+  std::vector<double> A((size_t)std::max(row_base, 1) * 8);
+  if (row_base > 0)
+    VQC_CK(cudaMemcpyAsync(A.data(), h->accbuf, sizeof(double) * 8 * row_base, cudaMemcpyDeviceToHost, h->stream));
+  VQC_CK(cudaStreamSynchronize(h->stream));
+  for (const AccRef& a : accs) {
+    const double* r = &A[(size_t)a.row * 8];
+    const cd Av[4] = {cd(r[0], r[1]), cd(r[2], r[3]), cd(r[4], r[5]), cd(r[6], r[7])};
+    for (const PGrad& pg : a.op.grads) {
+      double g = 0;
+      for (size_t i = 0; i < pg.D.size() && i < 4; ++i) {
+        // U1: D is 2x2 row-major and A[a][b] is stored at 2a+b; AccD: D is the
+        // diagonal bins and A's bins are stored in order
+        g += (pg.D[i] * Av[i]).real();
+      }
+      grads[pg.param] = g;
+    }
+  }
+  return VQC_OK;
+}
+
+int reverse_sweep_fused(vqc_state h, void* lam, void* y, const std::vector<GateSpec>& specs,
+                        const std::vector<std::vector<ParamInfo>>& params, double* grads) {
+  return h->dtype == VQC_C64 ? reverse_impl<float, 12>(h, lam, y, specs, params, grads)
+                             : reverse_impl<double, 11>(h, lam, y, specs, params, grads);
 }
 
 }  // namespace vqc

@@ -286,6 +286,7 @@ int vqc_state_destroy(vqc_state h) {
   for (void* w : h->work)
     if (w) cudaFree(w);
   if (h->accbuf) cudaFree(h->accbuf);
+  if (h->fused_scratch) cudaFree(h->fused_scratch);
   cudaFree(h->scr.partials);
   cudaFree(h->scr.counter);
   cudaFree(h->scr.result);
