@@ -154,6 +154,9 @@ struct ProfScope {
   ~ProfScope();
   cudaStream_t stream;
 };
+// Adds `count` to a counter class of the profile (no timing), e.g. the
+// number of passes and stages the planner produced.
+void prof_note(const char* cls, long long count);
 }  // namespace vqc
 
 // ----------------------------------------------------------------------------- grid reduction

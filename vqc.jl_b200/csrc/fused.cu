@@ -48,22 +48,26 @@ struct DevPass {
 };
 
 struct DevStage {
-  uint32_t dep[16];   // tile index of register slot j (OR with the thread part)
-  uint32_t thr_mask;  // tile bits held by the thread index, ascending
+  uint32_t dep[16];    // tile index of register slot j (OR with the thread part)
+  int64_t gdep[16];    // global offset of register slot j
+  uint64_t gthr_mask;  // global qubits of the thread's tile bits
+  uint32_t thr_mask;   // tile bits held by the thread index, ascending
   int32_t op_begin, op_end, pad;
 };
 
-struct DevOp {
-  int32_t type;
-  int32_t r0, r1;  // register slots of the targets (U1: r0; U2: r0 < r1, matrix bit 0 <-> r0)
-  int32_t slot;    // accumulation slot or -1
+// code: bits 0-3 op type, 4-5 r0, 6-7 r1, 8 tile-bit controls, 9 non-tile
+// controls, 10 accumulate.  The first 16 bytes are read as one vector load.
+struct alignas(16) DevOp {
+  int32_t code;
+  int32_t mat;     // pool offset (complex elements)
   uint32_t cmask, cval;  // controls on tile bits
   uint64_t gmask, gval;  // controls on non-tile qubits
-  int32_t mat;     // pool offset (complex elements)
+  int32_t slot;    // accumulation slot or -1
   int32_t nd;      // diagonal ops: number of qubits
   int32_t dbit[5];  // tile bit of diagonal qubit i, or -1
   int32_t dglob[5]; // global qubit of diagonal qubit i when not a tile bit
 };
+constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
 
 // ----------------------------------------------------------------------------- device helpers
 template <class R>
@@ -149,7 +153,7 @@ __device__ __forceinline__ void flush_acc(const R (&a)[8], double* sacc, int slo
 }
 
 // one-qubit op on register slot RR, both states in ADJ mode
-template <int RR, bool ADJ, class R>
+template <int RR, bool ADJ, bool CTL, class R>
 __device__ __forceinline__ void op_u1(cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm, uint32_t cv,
                                       uint32_t tthr, const uint32_t (&dep)[16], bool acc, double* sacc, int slot,
                                       int nwarps) {
@@ -160,7 +164,7 @@ __device__ __forceinline__ void op_u1(cplx<R> (&v)[16], cplx<R> (&w)[16], const 
 #pragma unroll
   for (int p = 0; p < 8; ++p) {
     const int j0 = ((p >> RR) << (RR + 1)) | (p & ((1 << RR) - 1)), j1 = j0 | (1 << RR);
-    if (((tthr | dep[j0]) & cm) == cv) {
+    if (!CTL || ((tthr | dep[j0]) & cm) == cv) {
       const cplx<R> x0 = v[j0], x1 = v[j1];
       v[j0] = cfma(u01, x1, cmul(u00, x0));
       v[j1] = cfma(u11, x1, cmul(u10, x0));
@@ -220,14 +224,18 @@ __device__ __forceinline__ void op_u2(cplx<R> (&v)[16], cplx<R> (&w)[16], const 
 }
 
 template <bool ADJ, class R>
-__device__ __forceinline__ void dispatch_u1(int r, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm,
-                                            uint32_t cv, uint32_t tthr, const uint32_t (&dep)[16], bool acc,
-                                            double* sacc, int slot, int nwarps) {
-  switch (r) {
-    case 0: op_u1<0, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 1: op_u1<1, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 2: op_u1<2, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    default: op_u1<3, ADJ, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+__device__ __forceinline__ void dispatch_u1(int r, bool ctl, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U,
+                                            uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t (&dep)[16],
+                                            bool acc, double* sacc, int slot, int nwarps) {
+  switch (r + (ctl ? 4 : 0)) {
+    case 0: op_u1<0, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 1: op_u1<1, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 2: op_u1<2, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 3: op_u1<3, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 4: op_u1<0, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 5: op_u1<1, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 6: op_u1<2, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    default: op_u1<3, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
   }
 }
 
@@ -261,49 +269,49 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 2)
   __syncthreads();
   const int nslots = ADJ ? P.nslots : 0;
   for (int i = threadIdx.x; i < nslots * NW * 8; i += NT) sacc[i] = 0;
-  const int64_t gthr = dep64(threadIdx.x, P.lo_qmask);
   C v[16], w[16];
+  const int s_first = P.stage_begin, s_last = P.stage_end - 1;
   for (int64_t tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
     const int64_t base = dep64(tile, P.nontile_mask);
-    // HBM -> shared (coalesced: consecutive threads hold consecutive low tile bits)
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const int64_t gi = base + gthr + P.dep_hi[k];
-      v[k] = psi[gi];
-      if (ADJ) w[k] = lam[gi];
-    }
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const uint32_t t = Swz<R>::f(threadIdx.x + k * NT);
-      sp[t] = v[k];
-      if (ADJ) sl[t] = w[k];
-    }
-    __syncthreads();
-    for (int s = P.stage_begin; s < P.stage_end; ++s) {
+    for (int s = s_first; s <= s_last; ++s) {
       const DevStage* S = stages + s;
       uint32_t dep[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) dep[j] = __ldg(&S->dep[j]);
       const uint32_t tthr = dep32(threadIdx.x, __ldg(&S->thr_mask));
+      if (s == s_first) {
+        // HBM -> registers directly in this stage's layout
+        const int64_t g0 = base + dep64(threadIdx.x, __ldg(&S->gthr_mask));
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const uint32_t t = Swz<R>::f(tthr | dep[j]);
-        v[j] = sp[t];
-        if (ADJ) w[j] = sl[t];
+        for (int j = 0; j < 16; ++j) {
+          const int64_t gi = g0 + __ldg(&S->gdep[j]);
+          v[j] = psi[gi];
+          if (ADJ) w[j] = lam[gi];
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const uint32_t t = Swz<R>::f(tthr | dep[j]);
+          v[j] = sp[t];
+          if (ADJ) w[j] = sl[t];
+        }
       }
       const int ob = __ldg(&S->op_begin), oe = __ldg(&S->op_end);
       for (int o = ob; o < oe; ++o) {
         const DevOp* op = ops + o;
-        const int type = __ldg(&op->type);
-        const uint64_t gm = __ldg(&op->gmask);
-        if ((base & (int64_t)gm) != (int64_t)__ldg(&op->gval)) continue;  // a non-tile control is off
-        const uint32_t cm = __ldg(&op->cmask), cv = __ldg(&op->cval);
-        const C* U = pool + __ldg(&op->mat);
+        const int4 hd = __ldg(reinterpret_cast<const int4*>(op));
+        const int code = hd.x, type = code & 15;
+        if (code & kCodeGCtl) {  // a control on a non-tile qubit: uniform over the tile
+          if ((base & (int64_t)__ldg(&op->gmask)) != (int64_t)__ldg(&op->gval)) continue;
+        }
+        const uint32_t cm = (uint32_t)hd.z, cv = (uint32_t)hd.w;
+        const C* U = pool + hd.y;
         if (type == kOpU1) {
-          const int slot = __ldg(&op->slot);
-          dispatch_u1<ADJ, R>(__ldg(&op->r0), v, w, U, cm, cv, tthr, dep, ADJ && slot >= 0, sacc, slot, NW);
+          const bool acc = ADJ && (code & kCodeAcc);
+          dispatch_u1<ADJ, R>((code >> 4) & 3, code & kCodeCtl, v, w, U, cm, cv, tthr, dep, acc, sacc,
+                              acc ? __ldg(&op->slot) : 0, NW);
         } else if (type == kOpU2) {
-          dispatch_u2<ADJ, R>(__ldg(&op->r0), __ldg(&op->r1), v, w, U, cm, cv, tthr, dep);
+          dispatch_u2<ADJ, R>((code >> 4) & 3, (code >> 6) & 3, v, w, U, cm, cv, tthr, dep);
         } else {
           // diagonal: phase index from the op's qubits (tile bits per amplitude, others per tile)
           const int nd = __ldg(&op->nd);
@@ -351,28 +359,25 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 2)
           }
         }
       }
+      if (s == s_last) {
+        // registers -> HBM directly from this stage's layout
+        const int64_t g0 = base + dep64(threadIdx.x, __ldg(&S->gthr_mask));
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const uint32_t t = Swz<R>::f(tthr | dep[j]);
-        sp[t] = v[j];
-        if (ADJ) sl[t] = w[j];
+        for (int j = 0; j < 16; ++j) {
+          const int64_t gi = g0 + __ldg(&S->gdep[j]);
+          psi[gi] = v[j];
+          if (ADJ) lam[gi] = w[j];
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const uint32_t t = Swz<R>::f(tthr | dep[j]);
+          sp[t] = v[j];
+          if (ADJ) sl[t] = w[j];
+        }
       }
-      __syncthreads();
+      __syncthreads();  // also orders this tile's last shared reads before the next tile's writes
     }
-    // shared -> HBM
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const uint32_t t = Swz<R>::f(threadIdx.x + k * NT);
-      v[k] = sp[t];
-      if (ADJ) w[k] = sl[t];
-    }
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const int64_t gi = base + gthr + P.dep_hi[k];
-      psi[gi] = v[k];
-      if (ADJ) lam[gi] = w[k];
-    }
-    __syncthreads();
   }
   if (ADJ && nslots > 0) {
     __syncthreads();
@@ -804,18 +809,24 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
         s.dep[j] = t;
       }
       s.thr_mask = ((1u << M) - 1) & ~rsmask;
+      s.gthr_mask = 0;
+      for (int b = 0; b < M; ++b)
+        if (s.thr_mask >> b & 1) s.gthr_mask |= 1ull << p.tile_q[b];
+      for (int j = 0; j < 16; ++j) {
+        int64_t g = 0;
+        for (int b = 0; b < M; ++b)
+          if (s.dep[j] >> b & 1) g |= int64_t(1) << p.tile_q[b];
+        s.gdep[j] = g;
+      }
       s.op_begin = (int)dops.size();
       for (int oi : st.ops) {
         const FOp& f = p.ops[oi];
         DevOp o{};
-        o.type = f.kind;
+        o.code = f.kind;
         o.slot = -1;
         auto slot_of = [&](int b) { return (int)(std::find(st.rs.begin(), st.rs.end(), b) - st.rs.begin()); };
-        if (f.kind == kOpU1) o.r0 = slot_of(tbit[f.tq[0]]);
-        if (f.kind == kOpU2) {
-          o.r0 = slot_of(tbit[f.tq[0]]);
-          o.r1 = slot_of(tbit[f.tq[1]]);
-        }
+        if (f.kind == kOpU1) o.code |= slot_of(tbit[f.tq[0]]) << 4;
+        if (f.kind == kOpU2) o.code |= (slot_of(tbit[f.tq[0]]) << 4) | (slot_of(tbit[f.tq[1]]) << 6);
         for (int q = 0; q < n; ++q) {
           if (!(f.cmask >> q & 1)) continue;
           const bool v = f.cval >> q & 1;
@@ -827,6 +838,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
             if (v) o.gval |= 1ull << q;
           }
         }
+        if (o.cmask) o.code |= kCodeCtl;
+        if (o.gmask) o.code |= kCodeGCtl;
         o.mat = (int)pool.size();
         for (const cd& c : f.mat) pool.push_back(mkc<R>((R)c.real(), (R)c.imag()));
         o.nd = f.nd;
@@ -846,12 +859,13 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
             // the accumulation runs as its own op right after the diagonal
             dops.push_back(o);
             DevOp a = o;
-            a.type = kOpAccD;
+            a.code = (a.code & ~15) | kOpAccD;
             dops.push_back(a);
             if (accs) accs->push_back(AccRef{row + o.slot, f});
             continue;
           }
           if (accs) accs->push_back(AccRef{row + o.slot, f});
+          o.code |= kCodeAcc;
         }
         dops.push_back(o);
       }
@@ -881,6 +895,22 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     locs[pi].stages = d.put(ds.data(), ds.size());
     // op indices in stages are local to this pass's op array
     locs[pi].ops = d.put(dops.data(), std::max<size_t>(dops.size(), 1));
+  }
+  {
+    long long np = 0, ns = 0, no = 0, nsa = 0;
+    for (auto& p : passes) {
+      if (p.standalone) {
+        ++nsa;
+        continue;
+      }
+      ++np;
+      ns += (long long)p.stages.size();
+      no += (long long)p.ops.size();
+    }
+    prof_note(ADJ ? "plan_adjoint_passes" : "plan_forward_passes", np);
+    prof_note(ADJ ? "plan_adjoint_stages" : "plan_forward_stages", ns);
+    prof_note(ADJ ? "plan_adjoint_ops" : "plan_forward_ops", no);
+    prof_note("plan_standalone_gates", nsa);
   }
   const size_t pool_off = d.put(pool.data(), std::max<size_t>(pool.size(), 1));
   int rc = upload_ops(h, d.buf.data(), d.buf.size());

@@ -119,6 +119,20 @@ ProfScope::~ProfScope() {
   if (token < (int)g_prof.size()) cudaEventRecord(g_prof[token].b, stream);
 }
 
+void prof_note(const char* cls, long long count) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on) return;
+  for (auto& x : g_prof_sum)
+    if (x.cls == cls) {
+      x.launches += count;
+      return;
+    }
+  ProfSum t;
+  t.cls = cls;
+  t.launches = count;
+  g_prof_sum.push_back(t);
+}
+
 static void prof_collect() {
   for (auto& r : g_prof) {
     float ms = 0;
