@@ -322,6 +322,122 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- secondary workloads
+def _events(stream):
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_gates_n30(args, local_rank):
+    """30 qubits: per-gate-class HBM GB/s of single gates, and the fused-block
+    speedup of 10 layers of (U3 on every qubit, CZ brickwork, one Toffoli)."""
+    import torch
+    import vqcb200 as V
+    from vqcb200 import _lib
+    from vqcb200 import workloads as W
+    torch.cuda.set_device(local_rank)
+    lib = V.load()
+    hbm, peak_kind = peaks()
+    n = args.qubits or 30
+    out = {"metric": "HBM GB/s per gate class and fused-block speedup, n=%d" % n, "unit": "GB/s", "n_gpus": 1,
+           "config": {"workload": "10 x (U3 on every qubit, CZ brickwork, 1 Toffoli), n=%d" % n}, "classes": {}}
+    spec = W.u3_cz_toffoli_spec(n, 10, SEED)
+    circuit = W.to_circuit(spec)
+    for dtype, name in ((np.complex128, "c128"), (np.complex64, "c64")):
+        psi = V.StateVector(n, dtype=dtype, device=local_rank)
+        V.apply(W.to_circuit(spec[:n]), psi)  # a dense state
+        stream = torch.cuda.ExternalStream(lib.vqc_state_stream(psi.handle), device=local_rank)
+        gates = {"u3_q1": V.U3Gate(1, 0.3, 0.2, 0.1), "u3_q%d" % n: V.U3Gate(n, 0.3, 0.2, 0.1),
+                 "cz": V.CZGate(n // 2, n // 2 + 1), "toffoli": V.TOFFOLIGate(2, n - 1, n // 2),
+                 "cnot": V.CNOTGate(3, n - 2), "crx": V.CRxGate(n - 3, 4, 0.4), "dense2q": V.QuantumGate((5, n - 4),
+                 np.linalg.qr(np.random.default_rng(1).standard_normal((4, 4)) + 0j)[0])}
+        res = {}
+        for gname, g in gates.items():
+            for _ in range(2):
+                V.apply(g, psi)
+            _lib.profile_enable(True)
+            a, b = _events(stream)
+            reps = max(1, args.steps)
+            a.record(stream)
+            for _ in range(reps):
+                V.apply(g, psi)
+            b.record(stream)
+            b.synchronize()
+            prof = _lib.profile_read()
+            _lib.profile_enable(False)
+            ms = a.elapsed_time(b) / reps
+            (cls, (nl, tms, tby)), = [(k, v) for k, v in prof.items() if not k.startswith("plan_")]
+            res[gname] = {"kernel": cls, "ms": ms, "algorithmic_bytes": tby / nl, "GB/s": tby / nl / (ms * 1e-3) / 1e9,
+                          "frac_of_hbm": tby / nl / (ms * 1e-3) / 1e9 / hbm,
+                          "full_pass_GB/s": 2 * (1 << n) * psi.dtype.itemsize / (ms * 1e-3) / 1e9}
+        # the whole circuit: one by one vs fused
+        times = {}
+        for fuse in (False, True):
+            V.apply(circuit, psi, fuse=fuse)
+            a, b = _events(stream)
+            a.record(stream)
+            V.apply(circuit, psi, fuse=fuse)
+            b.record(stream)
+            b.synchronize()
+            times["fused" if fuse else "unfused"] = a.elapsed_time(b)
+        ngates = len(circuit)
+        S = (1 << n) * psi.dtype.itemsize
+        res["circuit"] = {"gates": ngates, "unfused_ms": times["unfused"], "fused_ms": times["fused"],
+                          "fused_speedup": times["unfused"] / times["fused"],
+                          "effective_GB/s_fused": ngates * 2 * S / (times["fused"] * 1e-3) / 1e9,
+                          "note": "effective GB/s counts 2 x state bytes per gate; it can exceed the HBM roofline"}
+        out["classes"][name] = res
+        del psi
+    out["peak"] = {"hbm_GB/s": hbm, "kind": peak_kind}
+    print(json.dumps(out), flush=True)
+
+
+def run_dm_n13(args, local_rank):
+    """Density matrix, 13 qubits (1 GiB complex128): seeded random pure state,
+    8 layers of U3 on every qubit + CNOT ladder as rho <- U rho U^dagger,
+    partial trace over the top 4 qubits, basis probabilities."""
+    import torch
+    import vqcb200 as V
+    from vqcb200 import workloads as W
+    torch.cuda.set_device(local_rank)
+    lib = V.load()
+    n = args.qubits or 13
+    rng = np.random.default_rng(SEED)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    spec = W.u3_cnot_spec(n, 8, SEED)
+    circuit = W.to_circuit(spec)
+    res = {}
+    for fuse in (False, True):
+        rho = V.DensityMatrix(V.StateVector(psi))
+        V.apply(circuit, rho, fuse=fuse)  # warm-up
+        rho = V.DensityMatrix(V.StateVector(psi))
+        stream = torch.cuda.ExternalStream(lib.vqc_state_stream(rho.handle), device=local_rank)
+        a, b = _events(stream)
+        a.record(stream)
+        V.apply(circuit, rho, fuse=fuse)
+        b.record(stream)
+        b.synchronize()
+        res["fused" if fuse else "unfused"] = a.elapsed_time(b)
+    sites = list(range(n - 3, n + 1))
+    t0 = time.perf_counter()
+    red = V.partial_tr(rho, sites)
+    t_ptrace = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    probs = V.probabilities(rho)
+    t_probs = time.perf_counter() - t0
+    S = (1 << (2 * n)) * 16
+    out = {"metric": "density-matrix circuit time, n=%d (rho %d MiB)" % (n, S >> 20), "unit": "ms",
+           "config": {"workload": "8 x (U3 on every qubit + CNOT ladder) on rho, ptrace of the top 4 qubits, "
+                                  "probabilities", "gates": len(circuit)},
+           "circuit_ms_one_by_one": res["unfused"], "circuit_ms_fused": res["fused"],
+           "fused_speedup": res["unfused"] / res["fused"],
+           "one_by_one_GB/s_per_gate": len(circuit) * 2 * S / (res["unfused"] * 1e-3) / 1e9,
+           "ptrace_ms_host_call": t_ptrace * 1e3, "probs_ms_host_call": t_probs * 1e3,
+           "trace_of_reduced": float(np.trace(red).real), "sum_probs": float(probs.sum())}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,10 +447,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
+    ap.add_argument("--workload", default="adjoint", choices=["adjoint", "gates_n30", "dm_n13"],
+                    help="adjoint (the headline) or a secondary workload")
     ap.add_argument("--qubits", type=int, default=None,
                     help="state size (default 26, the headline; smaller sizes are for profiling captures)")
     args = ap.parse_args()
-    if args.qubits is not None:
+    if args.qubits is not None and args.workload == "adjoint":
         global N_QUBITS
         N_QUBITS = args.qubits
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -342,6 +460,12 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "gates_n30":
+        run_gates_n30(args, local_rank)
+        return
+    if args.workload == "dm_n13":
+        run_dm_n13(args, local_rank)
         return
     if world > 1:
         import datetime

@@ -140,3 +140,26 @@ def test_fused_deterministic():
     r2 = V.energy_and_gradient(H, c, V.StateVector(n, dtype=np.complex64))
     assert r1[0] == r2[0]
     assert np.array_equal(r1[1], r2[1])
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_fused_density_matrix_circuit(dtype):
+    """rho <- U rho U^dagger through the tile engine (U on the row qubits and
+    conj(U) on the column qubits as gates of the 2n-qubit vector)."""
+    n, layers = 7, 3
+    rng = np.random.default_rng(31)
+    psi = rand_psi(rng, n)
+    spec = W.u3_cnot_spec(n, layers, 5) + [("toffoli", (1, 4, 6), ()), ("cz", (2, 7), ()),
+                                            ("crx", (5, 3), (0.7,))]
+    rho = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
+    V.apply(W.to_circuit(spec), rho)
+    ref = O.density_matrix(psi)
+    O.dm_apply_circuit(ref, n, O.from_spec(spec))
+    assert max_abs(rho.data(), ref) < tol(dtype) * 100
+    red = V.partial_tr(rho, [6, 7])
+    assert max_abs(red.reshape(-1, order="F"), O.dm_ptrace(ref, n, [5, 6])) < tol(dtype) * 100
+    assert max_abs(V.probabilities(rho), O.dm_probs(ref, n)) < tol(dtype) * 100
+    # fused and one-by-one agree
+    rho2 = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
+    V.apply(W.to_circuit(spec), rho2, fuse=False)
+    assert max_abs(rho.data(), rho2.data()) < tol(dtype) * 100

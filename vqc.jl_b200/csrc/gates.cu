@@ -167,6 +167,33 @@ int apply_gate_raw(vqc_state h, int k, const int* pos, const double* mat) {
 int apply_circuit_raw(vqc_state h, const vqc_gate* gates, int ngates, const double* mats, bool dm, int fuse) {
   if (ngates < 0 || (ngates > 0 && (!gates || !mats))) return fail(VQC_ERR_ARG, "bad circuit arrays");
   if (fuse && !dm) return apply_circuit_fused(h, gates, ngates, mats);
+  if (fuse && dm) {
+    // rho <- U rho U^dagger is U on the row qubits and conj(U) on the column
+    // qubits (generic.jl:54-64); as gates of the 2n-qubit vector both go to the
+    // tile engine, which applies them (and the neighbouring gates) in one pass.
+    const int n = h->n_dm;
+    std::vector<vqc_gate> g2;
+    std::vector<double> m2;
+    g2.reserve(2 * (size_t)ngates);
+    for (int i = 0; i < ngates; ++i) {
+      const vqc_gate& gt = gates[i];
+      if (gt.nq < 1) return fail(VQC_ERR_ARG, "gate needs at least one position");
+      if (gt.nq > 5) return fail(VQC_ERR_UNSUPPORTED, "only implement 5-qubit gates and less currently.");
+      const size_t len = (size_t)2 << (2 * gt.nq);
+      vqc_gate a = gt, b = gt;
+      for (int j = 0; j < gt.nq; ++j) {
+        if (gt.pos[j] < 0 || gt.pos[j] >= n) return fail(VQC_ERR_ARG, "gate position out of range");
+        b.pos[j] = gt.pos[j] + n;
+      }
+      a.mat = (int64_t)m2.size();
+      m2.insert(m2.end(), mats + gt.mat, mats + gt.mat + len);
+      b.mat = (int64_t)m2.size();
+      for (size_t e = 0; e < len; ++e) m2.push_back(e & 1 ? -mats[gt.mat + e] : mats[gt.mat + e]);
+      g2.push_back(a);
+      g2.push_back(b);
+    }
+    return apply_circuit_fused(h, g2.data(), (int)g2.size(), m2.data());
+  }
   for (int i = 0; i < ngates; ++i) {
     const vqc_gate& gt = gates[i];
     int rc = dm ? dm_apply_gate_raw(h, gt.nq, gt.pos, mats + gt.mat) : apply_gate_raw(h, gt.nq, gt.pos, mats + gt.mat);
