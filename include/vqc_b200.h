@@ -56,12 +56,18 @@ typedef struct {
   int64_t mat;
 } vqc_gate;
 
-/* One circuit parameter: derivative dU/dtheta of gate `gate`, at mats + dmat. */
+/* One circuit parameter of gate `gate`; its matrix at mats + dmat is
+ *   kind VQC_PARAM_DERIVATIVE (0): dU/dtheta, or
+ *   kind VQC_PARAM_GENERATOR  (1): the gate G that QuantumCircuits'
+ *     differentiate(gate) returns, used by the reference as
+ *     grad = real(expectation(y_in, G, delta_in)) (circuitdiff.jl:29). */
 typedef struct {
   int32_t gate;
-  int32_t reserved;
+  int32_t kind;
   int64_t dmat;
 } vqc_param;
+#define VQC_PARAM_DERIVATIVE 0
+#define VQC_PARAM_GENERATOR 1
 
 /* One Pauli string coeff * prod_q P_q, P_q = I, X, Z, Y for (x_q, z_q) =
  * (0,0), (1,0), (0,1), (1,1): x bit q of xmask, z bit q of zmask. */

@@ -187,11 +187,21 @@ static int reverse_sweep(vqc_state h, void* lam, void* y, const vqc_gate* gates,
     if (rc) return rc;
     const GateSpec& gs = specs[i];
     const int d = 1 << gs.k;
-    for (ParamInfo& pi : per_gate[i]) {  // D_j = U^dagger dU_j (gs.U holds U^dagger)
+    for (ParamInfo& pi : per_gate[i]) {
       int sp[5];
       std::vector<cd> dU;
-      if ((rc = order_matrix(h->nq, gt.nq, gt.pos, mats + params[pi.index].dmat, sp, dU))) return rc;
+      const vqc_param& pr = params[pi.index];
+      if (pr.kind != VQC_PARAM_DERIVATIVE && pr.kind != VQC_PARAM_GENERATOR)
+        return fail(VQC_ERR_ARG, "unknown parameter kind");
+      if ((rc = order_matrix(h->nq, gt.nq, gt.pos, mats + pr.dmat, sp, dU))) return rc;
       pi.D.assign((size_t)d * d, cd(0));
+      if (pr.kind == VQC_PARAM_GENERATOR) {
+        // grad = Re <y_in|G|delta_in> = Re sum_ab conj(G_ba) A[a][b]: D = G^dagger
+        for (int r = 0; r < d; ++r)
+          for (int c = 0; c < d; ++c) pi.D[(size_t)r * d + c] = std::conj(dU[(size_t)c * d + r]);
+        continue;
+      }
+      // D_j = U^dagger dU_j (gs.U holds U^dagger)
       for (int r = 0; r < d; ++r)
         for (int c = 0; c < d; ++c) {
           cd acc = 0;

@@ -31,7 +31,7 @@ class Gate_t(ctypes.Structure):
 
 
 class Param_t(ctypes.Structure):
-    _fields_ = [("gate", ctypes.c_int32), ("reserved", ctypes.c_int32), ("dmat", ctypes.c_int64)]
+    _fields_ = [("gate", ctypes.c_int32), ("kind", ctypes.c_int32), ("dmat", ctypes.c_int64)]
 
 
 class Pauli_t(ctypes.Structure):
