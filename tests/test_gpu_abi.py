@@ -46,7 +46,8 @@ def test_generator_kind_matches_derivative_kind(n):
     arr, nt = H.packed()
     energy = (ctypes.c_double * 2)()
     g2 = np.zeros(p.nparams)
-    _lib.check(V.load().vqc_adjoint_grad(V.StateVector(n).handle, p.gates, p.ngates,
+    psi0 = V.StateVector(n)  # keep a reference: the handle lives as long as the object
+    _lib.check(V.load().vqc_adjoint_grad(psi0.handle, p.gates, p.ngates,
                                          mats.ctypes.data_as(_lib._D), p.params, p.nparams, arr, nt, energy,
                                          g2.ctypes.data_as(_lib._D)))
     assert abs(complex(energy[0], energy[1]) - e1) < 1e-12
@@ -61,13 +62,14 @@ def test_bad_parameter_kind_and_gate_index():
     energy = (ctypes.c_double * 2)()
     g = np.zeros(1)
     lib = V.load()
+    psi0 = V.StateVector(3)
     p.params[0].kind = 7
-    rc = lib.vqc_adjoint_grad(V.StateVector(3).handle, p.gates, p.ngates, p.mats_ptr(), p.params, 1, arr, nt, energy,
+    rc = lib.vqc_adjoint_grad(psi0.handle, p.gates, p.ngates, p.mats_ptr(), p.params, 1, arr, nt, energy,
                               g.ctypes.data_as(_lib._D))
     assert rc == -1
     p.params[0].kind = 0
     p.params[0].gate = 5
-    rc = lib.vqc_adjoint_grad(V.StateVector(3).handle, p.gates, p.ngates, p.mats_ptr(), p.params, 1, arr, nt, energy,
+    rc = lib.vqc_adjoint_grad(psi0.handle, p.gates, p.ngates, p.mats_ptr(), p.params, 1, arr, nt, energy,
                               g.ctypes.data_as(_lib._D))
     assert rc == -1
     assert b"out of range" in lib.vqc_last_error()

@@ -116,7 +116,8 @@ def test_gate_errors():
     m = np.eye(4, dtype=np.complex128).view(np.float64).ravel()
     assert lib.vqc_apply_gate(s.handle, 2, pos, m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == -1
     pos6 = (ctypes.c_int * 6)(*range(6))
-    assert lib.vqc_apply_gate(V.StateVector(6).handle, 6, pos6, m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == -4
+    s6 = V.StateVector(6)  # keep a reference: the handle lives as long as the object
+    assert lib.vqc_apply_gate(s6.handle, 6, pos6, m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == -4
 
 
 def test_single_qubit_register():

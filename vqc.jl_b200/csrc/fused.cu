@@ -36,18 +36,28 @@ namespace vqc {
 
 constexpr int kRegBits = 4;  // 16 amplitudes per thread
 constexpr int kMaxSlots = 64;
+constexpr int kMaxOpsPerPass = 192;  // bounds the pass's descriptors staged in shared memory
 enum { kOpU1 = 1, kOpU2 = 2, kOpDiag = 3, kOpAccD = 4 };
 
 struct DevPass {
-  int64_t dep_hi[16];     // global offset of the 4 top tile bits, per register index
   uint64_t nontile_mask;  // global bits enumerated by the tile counter
-  uint64_t lo_qmask;      // global qubits of tile bits 0..M-5 (the thread bits at load time)
   int64_t ntiles;
   int32_t stage_begin, stage_end;
-  int32_t nslots, pad;
+  int32_t nslots;
+  int32_t nops;           // ops of this pass (copied to shared memory with the stages)
+  int32_t npool;          // matrix pool entries of this pass
+  int32_t pad;
 };
 
-struct DevStage {
+// Shared-memory bytes of one pass: tiles, accumulation slots, and the pass's
+// own stage / op / matrix descriptors (read by every thread for every op, so
+// they are staged once per CTA instead of being fetched through L1/L2).
+template <class R, int M, bool ADJ>
+__host__ __device__ constexpr size_t tile_bytes() {
+  return (size_t)(ADJ ? 2 : 1) * (size_t(1) << M) * sizeof(cplx<R>);
+}
+
+struct alignas(16) DevStage {
   uint32_t dep[16];    // tile index of register slot j (OR with the thread part)
   int64_t gdep[16];    // global offset of register slot j
   uint64_t gthr_mask;  // global qubits of the thread's tile bits
@@ -104,7 +114,7 @@ __device__ __forceinline__ uint32_t dep32(uint32_t v, uint32_t mask) {
 
 template <class C>
 __device__ __forceinline__ C ldpool(const C* p) {
-  return __ldg(p);
+  return *p;
 }
 
 template <class R>
@@ -155,7 +165,7 @@ __device__ __forceinline__ void flush_acc(const R (&a)[8], double* sacc, int slo
 // one-qubit op on register slot RR, both states in ADJ mode
 template <int RR, bool ADJ, bool CTL, class R>
 __device__ __forceinline__ void op_u1(cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm, uint32_t cv,
-                                      uint32_t tthr, const uint32_t (&dep)[16], bool acc, double* sacc, int slot,
+                                      uint32_t tthr, const uint32_t* dep, bool acc, double* sacc, int slot,
                                       int nwarps) {
   const cplx<R> u00 = ldpool(U), u01 = ldpool(U + 1), u10 = ldpool(U + 2), u11 = ldpool(U + 3);
   R a[8];
@@ -182,7 +192,7 @@ __device__ __forceinline__ void op_u1(cplx<R> (&v)[16], cplx<R> (&w)[16], const 
 // two-qubit op on register slots (RA < RB), matrix bit 0 <-> RA
 template <int RA, int RB, bool ADJ, class R>
 __device__ __forceinline__ void op_u2(cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm, uint32_t cv,
-                                      uint32_t tthr, const uint32_t (&dep)[16]) {
+                                      uint32_t tthr, const uint32_t* dep) {
   cplx<R> m[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) m[i] = ldpool(U + i);
@@ -225,7 +235,7 @@ __device__ __forceinline__ void op_u2(cplx<R> (&v)[16], cplx<R> (&w)[16], const 
 
 template <bool ADJ, class R>
 __device__ __forceinline__ void dispatch_u1(int r, bool ctl, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U,
-                                            uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t (&dep)[16],
+                                            uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t* dep,
                                             bool acc, double* sacc, int slot, int nwarps) {
   switch (r + (ctl ? 4 : 0)) {
     case 0: op_u1<0, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
@@ -241,7 +251,7 @@ __device__ __forceinline__ void dispatch_u1(int r, bool ctl, cplx<R> (&v)[16], c
 
 template <bool ADJ, class R>
 __device__ __forceinline__ void dispatch_u2(int ra, int rb, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U,
-                                            uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t (&dep)[16]) {
+                                            uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t* dep) {
   switch (ra * 4 + rb) {
     case 1: op_u2<0, 1, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
     case 2: op_u2<0, 2, ADJ, R>(v, w, U, cm, cv, tthr, dep); break;
@@ -263,28 +273,45 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 2)
   extern __shared__ __align__(16) unsigned char smem[];
   C* sp = reinterpret_cast<C*>(smem);
   C* sl = sp + (ADJ ? T : 0);
-  double* sacc = reinterpret_cast<double*>(smem + (ADJ ? 2 : 1) * T * sizeof(C));
+  double* sacc = reinterpret_cast<double*>(smem + tile_bytes<R, M, ADJ>());
   __shared__ DevPass P;
   if (threadIdx.x == 0) P = *pass;
   __syncthreads();
   const int nslots = ADJ ? P.nslots : 0;
   for (int i = threadIdx.x; i < nslots * NW * 8; i += NT) sacc[i] = 0;
+  {
+    // stage this pass's descriptors in shared memory (16-byte words)
+    unsigned char* dst = smem + tile_bytes<R, M, ADJ>() + (size_t)nslots * NW * 8 * sizeof(double);
+    const int nst = P.stage_end - P.stage_begin;
+    const size_t b1 = sizeof(DevStage) * nst, b2 = sizeof(DevOp) * P.nops, b3 = sizeof(C) * P.npool;
+    const int4* s1 = reinterpret_cast<const int4*>(stages + P.stage_begin);
+    const int4* s2 = reinterpret_cast<const int4*>(ops);
+    const int4* s3 = reinterpret_cast<const int4*>(pool);
+    int4* d1 = reinterpret_cast<int4*>(dst);
+    int4* d2 = reinterpret_cast<int4*>(dst + b1);
+    int4* d3 = reinterpret_cast<int4*>(dst + b1 + b2);
+    for (size_t i = threadIdx.x; i < b1 / 16; i += NT) d1[i] = __ldg(s1 + i);
+    for (size_t i = threadIdx.x; i < b2 / 16; i += NT) d2[i] = __ldg(s2 + i);
+    for (size_t i = threadIdx.x; i < (b3 + 15) / 16; i += NT) d3[i] = __ldg(s3 + i);
+    stages = reinterpret_cast<const DevStage*>(dst) - P.stage_begin;
+    ops = reinterpret_cast<const DevOp*>(dst + b1);
+    pool = reinterpret_cast<const C*>(dst + b1 + b2);
+    __syncthreads();
+  }
   C v[16], w[16];
   const int s_first = P.stage_begin, s_last = P.stage_end - 1;
   for (int64_t tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
     const int64_t base = dep64(tile, P.nontile_mask);
     for (int s = s_first; s <= s_last; ++s) {
       const DevStage* S = stages + s;
-      uint32_t dep[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) dep[j] = __ldg(&S->dep[j]);
-      const uint32_t tthr = dep32(threadIdx.x, __ldg(&S->thr_mask));
+      const uint32_t* dep = S->dep;  // shared memory
+      const uint32_t tthr = dep32(threadIdx.x, (S->thr_mask));
       if (s == s_first) {
         // HBM -> registers directly in this stage's layout
-        const int64_t g0 = base + dep64(threadIdx.x, __ldg(&S->gthr_mask));
+        const int64_t g0 = base + dep64(threadIdx.x, (S->gthr_mask));
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const int64_t gi = g0 + __ldg(&S->gdep[j]);
+          const int64_t gi = g0 + (S->gdep[j]);
           v[j] = psi[gi];
           if (ADJ) w[j] = lam[gi];
         }
@@ -296,31 +323,31 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 2)
           if (ADJ) w[j] = sl[t];
         }
       }
-      const int ob = __ldg(&S->op_begin), oe = __ldg(&S->op_end);
+      const int ob = (S->op_begin), oe = (S->op_end);
       for (int o = ob; o < oe; ++o) {
         const DevOp* op = ops + o;
-        const int4 hd = __ldg(reinterpret_cast<const int4*>(op));
+        const int4 hd = *reinterpret_cast<const int4*>(op);
         const int code = hd.x, type = code & 15;
         if (code & kCodeGCtl) {  // a control on a non-tile qubit: uniform over the tile
-          if ((base & (int64_t)__ldg(&op->gmask)) != (int64_t)__ldg(&op->gval)) continue;
+          if ((base & (int64_t)(op->gmask)) != (int64_t)(op->gval)) continue;
         }
         const uint32_t cm = (uint32_t)hd.z, cv = (uint32_t)hd.w;
         const C* U = pool + hd.y;
         if (type == kOpU1) {
           const bool acc = ADJ && (code & kCodeAcc);
           dispatch_u1<ADJ, R>((code >> 4) & 3, code & kCodeCtl, v, w, U, cm, cv, tthr, dep, acc, sacc,
-                              acc ? __ldg(&op->slot) : 0, NW);
+                              acc ? (op->slot) : 0, NW);
         } else if (type == kOpU2) {
           dispatch_u2<ADJ, R>((code >> 4) & 3, (code >> 6) & 3, v, w, U, cm, cv, tthr, dep);
         } else {
           // diagonal: phase index from the op's qubits (tile bits per amplitude, others per tile)
-          const int nd = __ldg(&op->nd);
+          const int nd = (op->nd);
           uint32_t gidx = 0;
           int db[5];
 #pragma unroll
           for (int i = 0; i < 5; ++i) {
-            db[i] = i < nd ? __ldg(&op->dbit[i]) : -1;
-            if (i < nd && db[i] < 0) gidx |= (uint32_t)((base >> __ldg(&op->dglob[i])) & 1) << i;
+            db[i] = i < nd ? (op->dbit[i]) : -1;
+            if (i < nd && db[i] < 0) gidx |= (uint32_t)((base >> (op->dglob[i])) & 1) << i;
           }
           if (type == kOpDiag) {
 #pragma unroll
@@ -355,16 +382,16 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 2)
                   a[2 * b + 1] += im;
                 }
             }
-            flush_acc<R>(a, sacc, __ldg(&op->slot), NW);
+            flush_acc<R>(a, sacc, (op->slot), NW);
           }
         }
       }
       if (s == s_last) {
         // registers -> HBM directly from this stage's layout
-        const int64_t g0 = base + dep64(threadIdx.x, __ldg(&S->gthr_mask));
+        const int64_t g0 = base + dep64(threadIdx.x, (S->gthr_mask));
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const int64_t gi = g0 + __ldg(&S->gdep[j]);
+          const int64_t gi = g0 + (S->gdep[j]);
           psi[gi] = v[j];
           if (ADJ) lam[gi] = w[j];
         }
@@ -598,7 +625,7 @@ static void plan_passes(int n, const TileConfig& tc, bool adj, std::vector<PItem
       if (f.kind == kOpU1) need = 1ull << f.tq[0];
       if (f.kind == kOpU2) need = (1ull << f.tq[0]) | (1ull << f.tq[1]);
       const bool fits = popc64(Q | need) <= M;
-      const bool slot_ok = !(adj && f.acc) || p.nslots < kMaxSlots;
+      const bool slot_ok = (!(adj && f.acc) || p.nslots < kMaxSlots) && (int)p.ops.size() < kMaxOpsPerPass;
       if (!fits || !slot_ok) {
         blocked |= qs;
         continue;
@@ -737,11 +764,34 @@ struct Device {
   }
 };
 
+struct PassShape {
+  int nslots = 0, nstages = 0, nops = 0, npool = 0;
+};
+
+template <class R, int M, bool ADJ>
+static size_t pass_smem(const PassShape& ps) {
+  constexpr int NT = 1 << (M - kRegBits);
+  const size_t npool = (size_t)ps.npool * sizeof(cplx<R>);
+  return tile_bytes<R, M, ADJ>() + (ADJ ? (size_t)ps.nslots * (NT / 32) * 8 * sizeof(double) : 0) +
+         sizeof(DevStage) * ps.nstages + sizeof(DevOp) * ps.nops + ((npool + 15) & ~size_t(15));
+}
+
+template <class R, int M, bool ADJ>
+static int tile_grid(int device, const PassShape& ps) {
+  constexpr int NT = 1 << (M - kRegBits);
+  const size_t smem = pass_smem<R, M, ADJ>(ps);
+  auto kfun = k_tile<R, M, ADJ>;
+  cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, NT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  return device_info(device).sms * per_sm;
+}
+
 template <class R, int M, bool ADJ>
 static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, const DevStage* ds, const DevOp* dops,
-                       const void* pool, double* partials, int grid, int nslots) {
-  constexpr int NT = 1 << (M - kRegBits), T = 1 << M;
-  const size_t smem = (size_t)(ADJ ? 2 : 1) * T * sizeof(cplx<R>) + (ADJ ? (size_t)nslots * (NT / 32) * 8 * 8 : 0);
+                       const void* pool, double* partials, int grid, const PassShape& ps) {
+  constexpr int NT = 1 << (M - kRegBits);
+  const size_t smem = pass_smem<R, M, ADJ>(ps);
   auto kfun = k_tile<R, M, ADJ>;
   VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
   ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward",
@@ -749,17 +799,6 @@ static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, con
   kfun<<<grid, NT, smem, h->stream>>>((cplx<R>*)psi, (cplx<R>*)lam, dp, ds, dops, (const cplx<R>*)pool, partials);
   VQC_CK(cudaGetLastError());
   return VQC_OK;
-}
-
-template <class R, int M, bool ADJ>
-static int tile_grid(int device, int nslots) {
-  constexpr int NT = 1 << (M - kRegBits), T = 1 << M;
-  const size_t smem = (size_t)(ADJ ? 2 : 1) * T * sizeof(cplx<R>) + (ADJ ? (size_t)nslots * (NT / 32) * 8 * 8 : 0);
-  auto kfun = k_tile<R, M, ADJ>;
-  cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, NT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
-  return device_info(device).sms * per_sm;
 }
 
 int standalone_adjoint(vqc_state h, void* lam, void* y, const GateSpec& gs, bool acc, double* out);
@@ -782,6 +821,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   std::vector<cplx<R>> pool;
   struct Loc {
     size_t pass, stages, ops;
+    size_t pool_begin;  // in pool entries, a multiple of 16 bytes
+    PassShape shape;
     int nslots;
     int row0;
   };
@@ -798,6 +839,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     uint64_t tile_mask = 0;
     for (int q : p.tile_q) tile_mask |= 1ull << q;
     int slot = 0;
+    while ((pool.size() * sizeof(cplx<R>)) % 16) pool.push_back(mkc<R>(R(0), R(0)));
+    const size_t pool_begin = pool.size();
     for (const PlanStage& st : p.stages) {
       DevStage s{};
       uint32_t rsmask = 0;
@@ -840,7 +883,7 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
         }
         if (o.cmask) o.code |= kCodeCtl;
         if (o.gmask) o.code |= kCodeGCtl;
-        o.mat = (int)pool.size();
+        o.mat = (int)(pool.size() - pool_begin);
         for (const cd& c : f.mat) pool.push_back(mkc<R>((R)c.real(), (R)c.imag()));
         o.nd = f.nd;
         for (int i = 0; i < 5; ++i) {
@@ -875,16 +918,15 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     p.nslots = slot;
     DevPass P{};
     P.nontile_mask = ((n >= 64) ? ~0ull : ((1ull << n) - 1)) & ~tile_mask;
-    P.lo_qmask = 0;
-    for (int b = 0; b < M - kRegBits; ++b) P.lo_qmask |= 1ull << p.tile_q[b];
-    for (int k = 0; k < 16; ++k) {
-      int64_t off = 0;
-      for (int i = 0; i < kRegBits; ++i)
-        if (k >> i & 1) off |= int64_t(1) << p.tile_q[M - kRegBits + i];
-      P.dep_hi[k] = off;
-    }
     P.ntiles = int64_t(1) << (n - M);
     P.nslots = slot;
+    P.nops = (int)dops.size();
+    P.npool = (int)(pool.size() - pool_begin);
+    locs[pi].pool_begin = pool_begin;
+    locs[pi].shape.nslots = ADJ ? slot : 0;
+    locs[pi].shape.nstages = (int)ds.size();
+    locs[pi].shape.nops = P.nops;
+    locs[pi].shape.npool = P.npool;
     locs[pi].row0 = row;
     row += slot;
     locs[pi].nslots = slot;
@@ -912,7 +954,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     prof_note(ADJ ? "plan_adjoint_ops" : "plan_forward_ops", no);
     prof_note("plan_standalone_gates", nsa);
   }
-  const size_t pool_off = d.put(pool.data(), std::max<size_t>(pool.size(), 1));
+  for (int i = 0; i < 2; ++i) pool.push_back(mkc<R>(R(0), R(0)));  // the staging copy reads whole 16-byte words
+  const size_t pool_off = d.put(pool.data(), pool.size());
   int rc = upload_ops(h, d.buf.data(), d.buf.size());
   if (rc) return rc;
   const unsigned char* base = (const unsigned char*)h->opbuf;
@@ -920,7 +963,7 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   size_t need = 0;
   for (size_t pi = 0; pi < passes.size(); ++pi)
     if (!passes[pi].standalone && locs[pi].nslots > 0)
-      need = std::max(need, (size_t)tile_grid<R, M, ADJ>(h->device, locs[pi].nslots) * locs[pi].nslots * 8 *
+      need = std::max(need, (size_t)tile_grid<R, M, ADJ>(h->device, locs[pi].shape) * locs[pi].nslots * 8 *
                                 sizeof(double));
   double* partials = nullptr;
   if (ADJ && need > 0) {
@@ -947,10 +990,11 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
       continue;
     }
     const int nslots = locs[pi].nslots;
-    const int grid = tile_grid<R, M, ADJ>(h->device, nslots);
+    const int grid = tile_grid<R, M, ADJ>(h->device, locs[pi].shape);
     if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, (const DevPass*)(base + locs[pi].pass),
                                       (const DevStage*)(base + locs[pi].stages), (const DevOp*)(base + locs[pi].ops),
-                                      base + pool_off, partials, grid, nslots)))
+                                      base + pool_off + locs[pi].pool_begin * sizeof(cplx<R>), partials, grid,
+                                      locs[pi].shape)))
       return rc;
     if (ADJ && nslots > 0) {
       k_reduce_slots<<<nslots, 256, 0, h->stream>>>(partials, grid, nslots, locs[pi].row0, rows_dev);
