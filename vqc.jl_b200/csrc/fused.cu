@@ -78,6 +78,7 @@ struct alignas(16) DevOp {
   int32_t dglob[5]; // global qubit of diagonal qubit i when not a tile bit
 };
 constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
+// bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries accumulated
 
 // ----------------------------------------------------------------------------- device helpers
 template <class R>
@@ -163,89 +164,146 @@ __device__ __forceinline__ void flush_acc(const R (&a)[8], double* sacc, int slo
 }
 
 // one-qubit op on register slot RR, both states in ADJ mode
-template <int RR, bool ADJ, bool CTL, class R>
+// One-qubit matrix forms (read off the matrix on the host): general complex;
+// "RI" = real diagonal and imaginary off-diagonal (RX-like); real (RY-like);
+// diagonal (RZ / phase); the exact swap [[0,1],[1,0]] (X, the CNOT/Toffoli target).
+enum { kFormGen = 0, kFormRI = 1, kFormReal = 2, kFormDiag = 3, kFormSwap = 4 };
+// Reduced-matrix entries a parameter's D touches: all four, off-diagonal, diagonal.
+enum { kAccFull = 0, kAccOff = 1, kAccDiag = 2 };
+
+template <int FORM, class C>
+__device__ __forceinline__ void u1_apply(C& x0, C& x1, C u00, C u01, C u10, C u11) {
+  const C a = x0, b = x1;
+  if (FORM == kFormGen) {
+    x0 = cfma(u01, b, cmul(u00, a));
+    x1 = cfma(u11, b, cmul(u10, a));
+  } else if (FORM == kFormRI) {  // u00 = p, u01 = i q, u10 = i r, u11 = s (p, q, r, s real)
+    x0.x = fma(u00.x, a.x, -u01.y * b.y);
+    x0.y = fma(u00.x, a.y, u01.y * b.x);
+    x1.x = fma(u11.x, b.x, -u10.y * a.y);
+    x1.y = fma(u11.x, b.y, u10.y * a.x);
+  } else if (FORM == kFormReal) {
+    x0.x = fma(u00.x, a.x, u01.x * b.x);
+    x0.y = fma(u00.x, a.y, u01.x * b.y);
+    x1.x = fma(u10.x, a.x, u11.x * b.x);
+    x1.y = fma(u10.x, a.y, u11.x * b.y);
+  } else if (FORM == kFormDiag) {
+    x0 = cmul(u00, a);
+    x1 = cmul(u11, b);
+  } else {  // swap
+    x0 = b;
+    x1 = a;
+  }
+}
+
+template <int RR, bool ADJ, bool CTL, int FORM, class R>
 __device__ __forceinline__ void op_u1(cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm, uint32_t cv,
-                                      uint32_t tthr, const uint32_t* dep, bool acc, double* sacc, int slot,
+                                      uint32_t tthr, const uint32_t* dep, bool acc, int acck, double* sacc, int slot,
                                       int nwarps) {
-  const cplx<R> u00 = ldpool(U), u01 = ldpool(U + 1), u10 = ldpool(U + 2), u11 = ldpool(U + 3);
-  R a[8];
+  {
+    const cplx<R> u00 = ldpool(U), u01 = ldpool(U + 1), u10 = ldpool(U + 2), u11 = ldpool(U + 3);
 #pragma unroll
-  for (int i = 0; i < 8; ++i) a[i] = R(0);
-#pragma unroll
-  for (int p = 0; p < 8; ++p) {
-    const int j0 = ((p >> RR) << (RR + 1)) | (p & ((1 << RR) - 1)), j1 = j0 | (1 << RR);
-    if (!CTL || ((tthr | dep[j0]) & cm) == cv) {
-      const cplx<R> x0 = v[j0], x1 = v[j1];
-      v[j0] = cfma(u01, x1, cmul(u00, x0));
-      v[j1] = cfma(u11, x1, cmul(u10, x0));
-      if (ADJ) {
-        const cplx<R> y0 = w[j0], y1 = w[j1];
-        w[j0] = cfma(u01, y1, cmul(u00, y0));
-        w[j1] = cfma(u11, y1, cmul(u10, y0));
-        if (acc) acc_pair<R>(a, w[j0], w[j1], v[j0], v[j1]);
+    for (int p = 0; p < 8; ++p) {
+      const int j0 = ((p >> RR) << (RR + 1)) | (p & ((1 << RR) - 1)), j1 = j0 | (1 << RR);
+      if (!CTL || ((tthr | dep[j0]) & cm) == cv) {
+        u1_apply<FORM>(v[j0], v[j1], u00, u01, u10, u11);
+        if (ADJ) u1_apply<FORM>(w[j0], w[j1], u00, u01, u10, u11);
       }
     }
   }
-  if (ADJ && acc) flush_acc<R>(a, sacc, slot, nwarps);
+  if (ADJ && acc) {
+    // A[a][b] += conj(lam_a) psi_b over the pairs (after the uncompute); only
+    // the entries the parameters' D matrices touch
+    R a[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = R(0);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int j0 = ((p >> RR) << (RR + 1)) | (p & ((1 << RR) - 1)), j1 = j0 | (1 << RR);
+      if (!CTL || ((tthr | dep[j0]) & cm) == cv) {
+        const cplx<R> l0 = w[j0], l1 = w[j1], p0 = v[j0], p1 = v[j1];
+        if (acck != kAccOff) {
+          a[0] = fma(l0.x, p0.x, fma(l0.y, p0.y, a[0]));
+          a[1] = fma(l0.x, p0.y, fma(-l0.y, p0.x, a[1]));
+          a[6] = fma(l1.x, p1.x, fma(l1.y, p1.y, a[6]));
+          a[7] = fma(l1.x, p1.y, fma(-l1.y, p1.x, a[7]));
+        }
+        if (acck != kAccDiag) {
+          a[2] = fma(l0.x, p1.x, fma(l0.y, p1.y, a[2]));
+          a[3] = fma(l0.x, p1.y, fma(-l0.y, p1.x, a[3]));
+          a[4] = fma(l1.x, p0.x, fma(l1.y, p0.y, a[4]));
+          a[5] = fma(l1.x, p0.y, fma(-l1.y, p0.x, a[5]));
+        }
+      }
+    }
+    flush_acc<R>(a, sacc, slot, nwarps);
+  }
 }
 
 // two-qubit op on register slots (RA < RB), matrix bit 0 <-> RA
+template <class C>
+__device__ __forceinline__ void u2_quad(C& x0, C& x1, C& x2, C& x3, const C* U) {
+  const C x[4] = {x0, x1, x2, x3};
+  C o[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    o[r] = cmul(ldpool(U + 4 * r), x[0]);
+#pragma unroll
+    for (int c = 1; c < 4; ++c) o[r] = cfma(ldpool(U + 4 * r + c), x[c], o[r]);
+  }
+  x0 = o[0];
+  x1 = o[1];
+  x2 = o[2];
+  x3 = o[3];
+}
+
 template <int RA, int RB, bool ADJ, class R>
 __device__ __forceinline__ void op_u2(cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U, uint32_t cm, uint32_t cv,
                                       uint32_t tthr, const uint32_t* dep) {
-  cplx<R> m[16];
-#pragma unroll
-  for (int i = 0; i < 16; ++i) m[i] = ldpool(U + i);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    // insert zero bits at RA and RB into the 2-bit counter q
     int j = q;
     j = ((j >> RA) << (RA + 1)) | (j & ((1 << RA) - 1));
     j = ((j >> RB) << (RB + 1)) | (j & ((1 << RB) - 1));
     const int i0 = j, i1 = j | (1 << RA), i2 = j | (1 << RB), i3 = j | (1 << RA) | (1 << RB);
     if (((tthr | dep[i0]) & cm) == cv) {
-      cplx<R> x[4] = {v[i0], v[i1], v[i2], v[i3]};
-      cplx<R> o[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        o[r] = cmul(m[4 * r], x[0]);
-#pragma unroll
-        for (int c = 1; c < 4; ++c) o[r] = cfma(m[4 * r + c], x[c], o[r]);
-      }
-      v[i0] = o[0];
-      v[i1] = o[1];
-      v[i2] = o[2];
-      v[i3] = o[3];
-      if (ADJ) {
-        cplx<R> y[4] = {w[i0], w[i1], w[i2], w[i3]};
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          o[r] = cmul(m[4 * r], y[0]);
-#pragma unroll
-          for (int c = 1; c < 4; ++c) o[r] = cfma(m[4 * r + c], y[c], o[r]);
-        }
-        w[i0] = o[0];
-        w[i1] = o[1];
-        w[i2] = o[2];
-        w[i3] = o[3];
-      }
+      u2_quad(v[i0], v[i1], v[i2], v[i3], U);
+      if (ADJ) u2_quad(w[i0], w[i1], w[i2], w[i3], U);
     }
   }
 }
 
+template <int RR, bool ADJ, bool CTL, class R>
+__device__ __forceinline__ void dispatch_form(int form, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U,
+                                              uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t* dep, bool acc,
+                                              int acck, double* sacc, int slot, int nwarps) {
+  if (ADJ) {  // reverse sweep: the general and RX-like (CRX) forms
+    if (form == kFormRI)
+      op_u1<RR, ADJ, CTL, kFormRI, R>(v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps);
+    else
+      op_u1<RR, ADJ, CTL, kFormGen, R>(v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps);
+    return;
+  }
+  // forward: every form runs as the general one (a per-op form switch cost
+  // more than it saved in the single-state kernel)
+  (void)form;
+  op_u1<RR, ADJ, CTL, kFormGen, R>(v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps);
+}
+
 template <bool ADJ, class R>
-__device__ __forceinline__ void dispatch_u1(int r, bool ctl, cplx<R> (&v)[16], cplx<R> (&w)[16], const cplx<R>* U,
-                                            uint32_t cm, uint32_t cv, uint32_t tthr, const uint32_t* dep,
-                                            bool acc, double* sacc, int slot, int nwarps) {
+__device__ __forceinline__ void dispatch_u1(int r, bool ctl, int form, cplx<R> (&v)[16], cplx<R> (&w)[16],
+                                            const cplx<R>* U, uint32_t cm, uint32_t cv, uint32_t tthr,
+                                            const uint32_t* dep, bool acc, int acck, double* sacc, int slot,
+                                            int nwarps) {
   switch (r + (ctl ? 4 : 0)) {
-    case 0: op_u1<0, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 1: op_u1<1, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 2: op_u1<2, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 3: op_u1<3, ADJ, false, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 4: op_u1<0, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 5: op_u1<1, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    case 6: op_u1<2, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
-    default: op_u1<3, ADJ, true, R>(v, w, U, cm, cv, tthr, dep, acc, sacc, slot, nwarps); break;
+    case 0: dispatch_form<0, ADJ, false, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
+    case 1: dispatch_form<1, ADJ, false, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
+    case 2: dispatch_form<2, ADJ, false, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
+    case 3: dispatch_form<3, ADJ, false, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
+    case 4: dispatch_form<0, ADJ, true, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
+    case 5: dispatch_form<1, ADJ, true, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
+    case 6: dispatch_form<2, ADJ, true, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
+    default: dispatch_form<3, ADJ, true, R>(form, v, w, U, cm, cv, tthr, dep, acc, acck, sacc, slot, nwarps); break;
   }
 }
 
@@ -263,8 +321,15 @@ __device__ __forceinline__ void dispatch_u2(int ra, int rb, cplx<R> (&v)[16], cp
 }
 
 // The tile kernel: one launch per pass, persistent over the tiles.
+// Resident CTAs per SM the register budget is sized for (three resident
+// forward CTAs measured slower than two).
+template <class R, bool ADJ>
+struct MinBlocks {
+  static constexpr int value = 2;
+};
+
 template <class R, int M, bool ADJ>
-__global__ void __launch_bounds__(1 << (M - kRegBits), 2)
+__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
     k_tile(cplx<R>* __restrict__ psi, cplx<R>* __restrict__ lam, const DevPass* __restrict__ pass,
            const DevStage* __restrict__ stages, const DevOp* __restrict__ ops, const cplx<R>* __restrict__ pool,
            double* __restrict__ partials) {
@@ -335,8 +400,8 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), 2)
         const C* U = pool + hd.y;
         if (type == kOpU1) {
           const bool acc = ADJ && (code & kCodeAcc);
-          dispatch_u1<ADJ, R>((code >> 4) & 3, code & kCodeCtl, v, w, U, cm, cv, tthr, dep, acc, sacc,
-                              acc ? (op->slot) : 0, NW);
+          dispatch_u1<ADJ, R>((code >> 4) & 3, code & kCodeCtl, (code >> 11) & 7, v, w, U, cm, cv, tthr, dep, acc,
+                              (code >> 14) & 3, sacc, acc ? (op->slot) : 0, NW);
         } else if (type == kOpU2) {
           dispatch_u2<ADJ, R>((code >> 4) & 3, (code >> 6) & 3, v, w, U, cm, cv, tthr, dep);
         } else {
@@ -812,6 +877,30 @@ struct AccRef {
   FOp op;
 };
 
+// The structure class of a one-qubit matrix (exact zeros: the matrices are
+// built from closed forms, so structural zeros are exact).
+static int u1_form(const std::vector<cd>& m) {
+  const cd u00 = m[0], u01 = m[1], u10 = m[2], u11 = m[3];
+  if (u00 == cd(0) && u11 == cd(0) && u01 == cd(1) && u10 == cd(1)) return kFormSwap;
+  if (u01 == cd(0) && u10 == cd(0)) return kFormDiag;
+  if (u00.imag() == 0 && u01.imag() == 0 && u10.imag() == 0 && u11.imag() == 0) return kFormReal;
+  if (u00.imag() == 0 && u11.imag() == 0 && u01.real() == 0 && u10.real() == 0) return kFormRI;
+  return kFormGen;
+}
+
+// Which entries of the reduced matrix the op's parameters need.
+static int acc_kind(const FOp& f) {
+  bool diag = false, off = false;
+  for (const PGrad& pg : f.grads) {
+    if (pg.D.size() < 4) return kAccFull;
+    if (pg.D[0] != cd(0) || pg.D[3] != cd(0)) diag = true;
+    if (pg.D[1] != cd(0) || pg.D[2] != cd(0)) off = true;
+  }
+  if (diag && !off) return kAccDiag;
+  if (off && !diag) return kAccOff;
+  return kAccFull;
+}
+
 template <class R, int M, bool ADJ>
 static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
                     std::vector<AccRef>* accs, double* rows_dev) {
@@ -868,7 +957,11 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
         o.code = f.kind;
         o.slot = -1;
         auto slot_of = [&](int b) { return (int)(std::find(st.rs.begin(), st.rs.end(), b) - st.rs.begin()); };
-        if (f.kind == kOpU1) o.code |= slot_of(tbit[f.tq[0]]) << 4;
+        if (f.kind == kOpU1) {
+          o.code |= slot_of(tbit[f.tq[0]]) << 4;
+          o.code |= u1_form(f.mat) << 11;
+          if (ADJ && f.acc) o.code |= acc_kind(f) << 14;
+        }
         if (f.kind == kOpU2) o.code |= (slot_of(tbit[f.tq[0]]) << 4) | (slot_of(tbit[f.tq[1]]) << 6);
         for (int q = 0; q < n; ++q) {
           if (!(f.cmask >> q & 1)) continue;
