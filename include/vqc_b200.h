@@ -177,6 +177,36 @@ int vqc_dm_probs(vqc_state rho, double* out);
 /* tr(rho) (densitymatrix.jl:58), FP64 (re, im). */
 int vqc_dm_trace(vqc_state rho, double* out);
 
+/* ---- serving: continuous batching of many circuits on one GPU (no
+ *      counterpart in the reference, which evaluates one circuit per call) ----
+ * A server owns one GPU stream, a worker thread and `planner_threads`
+ * planning threads.  Requests start from |0...0>, run their circuit, and
+ * return expectation(H, circuit * psi0) and, if want_grad, its gradient (the
+ * same quantities as vqc_adjoint_grad).  Admission is by device memory: a
+ * request is admitted when its states, descriptors and scratch fit
+ * `memory_bytes` and fewer than `max_active` requests run.  Every loop
+ * iteration advances every admitted request by one step, all steps of a kind
+ * in one launch; requests arriving meanwhile join at the next iteration.  A
+ * request's result does not depend on the requests it is batched with. */
+typedef struct vqc_server_s* vqc_server;
+int vqc_serve_open(int device, int dtype, size_t memory_bytes, int max_active, int planner_threads,
+                   vqc_server* out);
+/* Queues one request (inputs are copied).  grads_out (nparams doubles) must
+ * stay valid until the request is finished.  Gates must have at most two
+ * target qubits (controls read off the matrix), 9..40 qubits. */
+int vqc_serve_submit(vqc_server s, int nqubits, const vqc_gate* gates, int ngates, const double* mats,
+                     const vqc_param* params, int nparams, const vqc_pauli* terms, int nterms, int want_grad,
+                     double* grads_out, int64_t* ticket);
+/* 0: not finished; 1: finished (energy and latency_s = completion - submission
+ * filled, the ticket is released); negative: the request failed. */
+int vqc_serve_poll(vqc_server s, int64_t ticket, double* energy, double* latency_s);
+/* As vqc_serve_poll but waits up to timeout_ms (then VQC_ERR_TIMEOUT). */
+int vqc_serve_wait(vqc_server s, int64_t ticket, int timeout_ms, double* energy, double* latency_s);
+/* out[0..6]: completed, loop iterations, launches, request-steps launched,
+ * device bytes admitted, requests running, requests waiting. */
+int vqc_serve_stats(vqc_server s, long long* out);
+int vqc_serve_close(vqc_server s);
+
 #ifdef __cplusplus
 }
 #endif

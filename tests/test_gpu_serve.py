@@ -1,0 +1,136 @@
+"""GPU tests of the serving loop: results of batched requests of mixed sizes
+against the single-request path and the FP64 oracle; the same result alone
+and in the mix; memory-based admission; errors."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import vqcb200 as V
+from helpers import rel
+from oracle import oracle as O
+from vqcb200 import workloads as W
+from vqcb200.serve import Server
+
+pytestmark = pytest.mark.gpu
+
+
+def make_request(rng, n, layers):
+    th = rng.uniform(0, 2 * np.pi, layers * 2 * n)
+    spec = W.hea_spec(n, layers, th)
+    g = float(rng.uniform(0.2, 1.5))
+    return spec, W.tfim_spec(n, g)
+
+
+def test_serve_matches_single_path_and_oracle():
+    rng = np.random.default_rng(50)
+    reqs = []
+    for i in range(24):
+        n = int(rng.integers(9, 17))
+        layers = int(rng.integers(2, 6))
+        spec, hspec = make_request(rng, n, layers)
+        reqs.append((n, spec, hspec, bool(i % 2)))
+    with Server(dtype=np.complex64, memory_bytes=1 << 30, max_active=64) as srv:
+        tickets = [srv.submit(n, W.to_circuit(spec), W.to_operator(h), want_grad=g) for n, spec, h, g in reqs]
+        results = [srv.wait(t) for t in tickets]
+        st = srv.stats()
+    assert st["completed"] == len(reqs)
+    # batching happened: fewer launches than request-steps
+    assert st["launches"] < st["request_steps"]
+    for (n, spec, hspec, g), (e, grads, lat) in zip(reqs, results):
+        e_ref, g_ref = O.energy_and_gradient(O.from_spec(spec), O.terms_from_spec(hspec), O.zero_state(n), nthreads=4)
+        assert abs(e - e_ref) / max(abs(e_ref), 1.0) < 1e-5
+        if g:
+            assert rel(grads, g_ref) < 1e-5
+        else:
+            assert grads is None
+        assert lat >= 0
+
+
+def test_same_result_alone_and_in_the_mix():
+    rng = np.random.default_rng(51)
+    mix = []
+    for i in range(16):
+        n = int(rng.integers(9, 19))
+        spec, hspec = make_request(rng, n, int(rng.integers(2, 7)))
+        mix.append((n, spec, hspec))
+    probe = mix[5]
+    with Server(dtype=np.complex64, memory_bytes=2 << 30, max_active=64) as srv:
+        t = srv.submit(probe[0], W.to_circuit(probe[1]), W.to_operator(probe[2]), want_grad=True)
+        alone = srv.wait(t)
+        ts = [srv.submit(n, W.to_circuit(s), W.to_operator(h), want_grad=True) for n, s, h in mix]
+        in_mix = [srv.wait(x) for x in ts][5]
+    assert alone[0] == in_mix[0]
+    assert np.array_equal(alone[1], in_mix[1])
+
+
+def test_requests_arriving_while_others_run():
+    """Continuous batching: a second wave submitted from another thread while
+    the first runs is admitted and finishes; everything completes."""
+    rng = np.random.default_rng(52)
+    reqs = []
+    for _ in range(40):
+        n = int(rng.integers(10, 20))
+        reqs.append((n,) + make_request(rng, n, int(rng.integers(2, 10))))
+    out = {}
+    with Server(dtype=np.complex64, memory_bytes=256 << 20, max_active=8) as srv:
+        def client(lo, hi, delay):
+            time.sleep(delay)
+            ts = [(i, srv.submit(reqs[i][0], W.to_circuit(reqs[i][1]), W.to_operator(reqs[i][2]))) for i in range(lo, hi)]
+            for i, t in ts:
+                out[i] = srv.wait(t)
+        th = [threading.Thread(target=client, args=(0, 20, 0.0)), threading.Thread(target=client, args=(20, 40, 0.05))]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        st = srv.stats()
+    assert len(out) == 40 and st["completed"] == 40
+    # the memory budget (256 MiB) and 8 slots forced waiting: more iterations than the longest request's steps
+    assert st["iterations"] > 0
+    for i in (0, 25, 39):
+        n, spec, hspec = reqs[i]
+        e_ref, g_ref = O.energy_and_gradient(O.from_spec(spec), O.terms_from_spec(hspec), O.zero_state(n), nthreads=4)
+        assert abs(out[i][0] - e_ref) / max(abs(e_ref), 1.0) < 1e-5
+        assert rel(out[i][1], g_ref) < 1e-5
+
+
+def test_fp64_server():
+    rng = np.random.default_rng(53)
+    n = 12
+    spec, hspec = make_request(rng, n, 3)
+    with Server(dtype=np.complex128, memory_bytes=1 << 28, max_active=4) as srv:
+        e, g, _ = srv.wait(srv.submit(n, W.to_circuit(spec), W.to_operator(hspec)))
+    e_ref, g_ref = O.energy_and_gradient(O.from_spec(spec), O.terms_from_spec(hspec), O.zero_state(n), nthreads=4)
+    assert abs(e - e_ref) < 1e-12
+    assert rel(g, g_ref) < 1e-12
+
+
+def test_admission_rejects_oversized_and_bad_requests():
+    rng = np.random.default_rng(54)
+    spec, hspec = make_request(rng, 20, 2)
+    with Server(dtype=np.complex64, memory_bytes=1 << 20, max_active=4) as srv:
+        t = srv.submit(20, W.to_circuit(spec), W.to_operator(hspec))
+        with pytest.raises(BlockingIOError):
+            srv.wait(t)
+        # three-target dense gates are not served
+        from oracle import gates_ref as GR
+        bad = V.QCircuit([V.QuantumGate((1, 2, 3), GR.random_unitary(3, rng))])
+        t = srv.submit(9, bad, V.QubitsOperator(V.pauli({1: "Z"})))
+        with pytest.raises(NotImplementedError):
+            srv.wait(t)
+        # a tiny request still works after the failures
+        spec, hspec = make_request(rng, 9, 1)
+        e, g, _ = srv.wait(srv.submit(9, W.to_circuit(spec), W.to_operator(hspec)))
+        assert np.isfinite(e.real)
+
+
+def test_wait_timeout():
+    rng = np.random.default_rng(55)
+    spec, hspec = make_request(rng, 22, 12)
+    with Server(dtype=np.complex64, memory_bytes=1 << 30, max_active=4) as srv:
+        t = srv.submit(22, W.to_circuit(spec), W.to_operator(hspec))
+        with pytest.raises(TimeoutError):
+            srv.wait(t, timeout=0.0)
+        srv.wait(t)

@@ -122,10 +122,6 @@ static int launch_adj_r(const GateSpec& gd, vqc_state h, void* lam, void* psi, b
   }
 }
 
-struct ParamInfo {
-  int index;          // position in the caller's params array
-  std::vector<cd> D;  // U^dagger dU/dtheta in sorted order (2^k x 2^k)
-};
 int fused_supported(vqc_state h);
 int reverse_sweep_fused(vqc_state h, void* lam, void* y, const std::vector<GateSpec>& specs,
                         const std::vector<std::vector<ParamInfo>>& params, double* grads);
@@ -169,21 +165,21 @@ int per_gate_params_grad(vqc_state h, void* lam, void* y, const GateSpec& gs, co
   return VQC_OK;
 }
 
-// The reverse sweep over lam (cotangent) and y (state): both are overwritten
-// with their values at the circuit input; grads[j] receive the partials.
-static int reverse_sweep(vqc_state h, void* lam, void* y, const vqc_gate* gates, int ngates, const double* mats,
-                         const vqc_param* params, int nparams, double* grads, bool fuse) {
-  if (nparams < 0 || (nparams > 0 && (!params || !grads))) return fail(VQC_ERR_ARG, "bad parameter arrays");
-  std::vector<std::vector<ParamInfo>> per_gate(ngates);
+// The analysed gates of a circuit for its reverse sweep (U^dagger) and, per
+// gate, its parameters with D = U^dagger dU/dtheta (or G^dagger).
+int prepare_reverse(int nq, const vqc_gate* gates, int ngates, const double* mats, const vqc_param* params,
+                    int nparams, std::vector<GateSpec>& specs, std::vector<std::vector<ParamInfo>>& per_gate) {
+  if (nparams < 0 || (nparams > 0 && !params)) return fail(VQC_ERR_ARG, "bad parameter arrays");
+  per_gate.assign(ngates, {});
   for (int j = 0; j < nparams; ++j) {
     const int gi = params[j].gate;
     if (gi < 0 || gi >= ngates) return fail(VQC_ERR_ARG, "parameter refers to a gate out of range");
     per_gate[gi].push_back(ParamInfo{j, {}});
   }
-  std::vector<GateSpec> specs(ngates);
+  specs.assign(ngates, GateSpec());
   for (int i = 0; i < ngates; ++i) {
     const vqc_gate& gt = gates[i];
-    int rc = analyze_gate(h->nq, gt.nq, gt.pos, mats + gt.mat, true, specs[i]);
+    int rc = analyze_gate(nq, gt.nq, gt.pos, mats + gt.mat, true, specs[i]);
     if (rc) return rc;
     const GateSpec& gs = specs[i];
     const int d = 1 << gs.k;
@@ -193,7 +189,7 @@ static int reverse_sweep(vqc_state h, void* lam, void* y, const vqc_gate* gates,
       const vqc_param& pr = params[pi.index];
       if (pr.kind != VQC_PARAM_DERIVATIVE && pr.kind != VQC_PARAM_GENERATOR)
         return fail(VQC_ERR_ARG, "unknown parameter kind");
-      if ((rc = order_matrix(h->nq, gt.nq, gt.pos, mats + pr.dmat, sp, dU))) return rc;
+      if ((rc = order_matrix(nq, gt.nq, gt.pos, mats + pr.dmat, sp, dU))) return rc;
       pi.D.assign((size_t)d * d, cd(0));
       if (pr.kind == VQC_PARAM_GENERATOR) {
         // grad = Re <y_in|G|delta_in> = Re sum_ab conj(G_ba) A[a][b]: D = G^dagger
@@ -210,6 +206,18 @@ static int reverse_sweep(vqc_state h, void* lam, void* y, const vqc_gate* gates,
         }
     }
   }
+  return VQC_OK;
+}
+
+// The reverse sweep over lam (cotangent) and y (state): both are overwritten
+// with their values at the circuit input; grads[j] receive the partials.
+static int reverse_sweep(vqc_state h, void* lam, void* y, const vqc_gate* gates, int ngates, const double* mats,
+                         const vqc_param* params, int nparams, double* grads, bool fuse) {
+  if (nparams > 0 && !grads) return fail(VQC_ERR_ARG, "bad parameter arrays");
+  std::vector<GateSpec> specs;
+  std::vector<std::vector<ParamInfo>> per_gate;
+  int rc0 = prepare_reverse(h->nq, gates, ngates, mats, params, nparams, specs, per_gate);
+  if (rc0) return rc0;
   if (fuse && fused_supported(h)) return reverse_sweep_fused(h, lam, y, specs, per_gate, grads);
   for (int i = ngates - 1; i >= 0; --i) {
     int rc = per_gate[i].empty() ? standalone_adjoint(h, lam, y, specs[i], false, nullptr)

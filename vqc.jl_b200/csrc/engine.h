@@ -39,6 +39,16 @@ int analyze_gate(int n, int k, const int* pos, const double* mat, bool dagger, G
 // Sorted-order matrix of an arbitrary operator (no unitarity assumed).
 int order_matrix(int n, int k, const int* pos, const double* mat, int* sp, std::vector<cd>& M);
 
+// One circuit parameter in the reverse sweep: D = U^dagger dU/dtheta (or
+// G^dagger for generator-kind parameters), sorted order, 2^k x 2^k.
+struct ParamInfo {
+  int index;  // position in the caller's params array
+  std::vector<cd> D;
+};
+
+int prepare_reverse(int nq, const vqc_gate* gates, int ngates, const double* mats, const vqc_param* params,
+                    int nparams, std::vector<GateSpec>& specs, std::vector<std::vector<ParamInfo>>& per_gate);
+
 // Applies an analysed gate to a 2^nq vector on `stream` (dtype VQC_C64/C128).
 int launch_gate(const GateSpec& g, void* v, int nq, int dtype, int device, cudaStream_t stream);
 

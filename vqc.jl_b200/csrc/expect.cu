@@ -16,18 +16,10 @@
 
 #include "engine.h"
 #include "subspace.cuh"
+#include "tile_plan.cuh"
 
 namespace vqc {
 
-struct DevTerm {
-  uint64_t z;
-  double2 c;  // coefficient for the expectation, times i^{popcount(x & z)}
-  double2 d;  // coefficient for the applied operator, same phase
-};
-struct DevGroup {
-  uint64_t x;
-  int start, count;
-};
 
 constexpr int kMaxTermsPerLaunch = 2048;
 
@@ -37,7 +29,7 @@ struct PauliPlan {
   std::vector<DevTerm> terms;
 };
 
-static int plan_pauli(int nq, const vqc_pauli* t, int nt, bool apply_hermitian_part, PauliPlan& p) {
+int plan_pauli(int nq, const vqc_pauli* t, int nt, bool apply_hermitian_part, PauliPlan& p) {
   if (nt < 0 || (nt > 0 && !t)) return fail(VQC_ERR_ARG, "bad Pauli term array");
   const uint64_t lim = nq >= 64 ? ~0ull : ((1ull << nq) - 1);
   std::map<uint64_t, std::vector<int>> by_x;
@@ -369,3 +361,116 @@ int vqc_apply_dense_add(vqc_state psi, vqc_state out, int k, const int* pos, con
 }
 
 }  // extern "C"
+
+namespace vqc {
+
+// ----------------------------------------------------------------------------- serving support
+int serve_pauli_image(int nq, const vqc_pauli* terms, int nterms, bool hermitian_part, std::vector<unsigned char>& img,
+                      int& ng, int& nt) {
+  if (nterms > kMaxTermsPerLaunch) return fail(VQC_ERR_UNSUPPORTED, "serving takes at most 2048 Pauli terms");
+  PauliPlan p;
+  int rc = plan_pauli(nq, terms, nterms, hermitian_part, p);
+  if (rc) return rc;
+  ng = (int)p.groups.size();
+  nt = (int)p.terms.size();
+  const size_t gb = sizeof(DevGroup) * p.groups.size(), tb = sizeof(DevTerm) * p.terms.size();
+  img.resize(gb + tb);
+  if (gb) std::memcpy(img.data(), p.groups.data(), gb);
+  if (tb) std::memcpy(img.data() + gb, p.terms.data(), tb);
+  return VQC_OK;
+}
+
+// One Pauli pass each over many states: item blockIdx.y, indices strided over
+// blockIdx.x; per-CTA FP64 partial sums of conj(psi) H psi in fixed order.
+template <class R, bool WRITE>
+__global__ void __launch_bounds__(kRedThreads) k_pauli_batch(const PauliItem* __restrict__ items) {
+  extern __shared__ unsigned char smem[];
+  __shared__ double red[kRedThreads / 32][2];
+  const PauliItem it = items[blockIdx.y];
+  if ((int64_t)blockIdx.x * blockDim.x >= it.N) return;  // beyond this state: no partial written
+  DevGroup* sg = reinterpret_cast<DevGroup*>(smem);
+  DevTerm* st = reinterpret_cast<DevTerm*>(smem + sizeof(DevGroup) * it.ng);
+  for (int i = threadIdx.x; i < it.ng; i += blockDim.x) sg[i] = it.groups[i];
+  for (int i = threadIdx.x; i < it.nt; i += blockDim.x) st[i] = it.terms[i];
+  __syncthreads();
+  const cplx<R>* ket = (const cplx<R>*)it.ket;
+  cplx<R>* out = (cplx<R>*)it.out;
+  double acc[2] = {0, 0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < it.N; i += stride) {
+    double2 hv = make_double2(0, 0), ov = make_double2(0, 0);
+    for (int gi = 0; gi < it.ng; ++gi) {
+      const DevGroup g = sg[gi];
+      const int64_t j = i ^ (int64_t)g.x;
+      const double2 kv = to_d2(ket[j]);
+      double2 f = make_double2(0, 0), fd = make_double2(0, 0);
+      for (int q = g.start; q < g.start + g.count; ++q) {
+        const double sgn = (__popcll((unsigned long long)j & st[q].z) & 1) ? -1.0 : 1.0;
+        f.x = fma(sgn, st[q].c.x, f.x);
+        f.y = fma(sgn, st[q].c.y, f.y);
+        if (WRITE) {
+          fd.x = fma(sgn, st[q].d.x, fd.x);
+          fd.y = fma(sgn, st[q].d.y, fd.y);
+        }
+      }
+      hv = cfma(f, kv, hv);
+      if (WRITE) ov = cfma(fd, kv, ov);
+    }
+    if (WRITE) out[i] = mkc<R>((R)ov.x, (R)ov.y);
+    const double2 b = to_d2(ket[i]);
+    acc[0] = fma(b.x, hv.x, fma(b.y, hv.y, acc[0]));
+    acc[1] = fma(b.x, hv.y, fma(-b.y, hv.x, acc[1]));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    double v = acc[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double v = 0;
+    for (int w = 0; w < kRedThreads / 32; ++w) v += red[w][threadIdx.x];
+    it.partials[blockIdx.x * 2 + threadIdx.x] = v;
+  }
+}
+
+__global__ void __launch_bounds__(32) k_pauli_reduce_batch(const PauliRed* __restrict__ items) {
+  const PauliRed it = items[blockIdx.x];
+  if (threadIdx.x < 2) {
+    double v = 0;
+    for (int b = 0; b < it.nblocks; ++b) v += it.partials[b * 2 + threadIdx.x];
+    it.out[threadIdx.x] = v;
+  }
+}
+
+int serve_launch_pauli(int dtype, bool write, const PauliItem* d_items, int nitems, int gridx, size_t smem,
+                       cudaStream_t stream) {
+  if (nitems == 0) return VQC_OK;
+  ProfScope prof(stream, "serve_pauli", 0);
+#define VQC_PB(R, W)                                                                                        \
+  do {                                                                                                      \
+    auto kf = k_pauli_batch<R, W>;                                                                          \
+    if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kf<<<dim3(gridx, nitems), kRedThreads, smem, stream>>>(d_items);                                        \
+  } while (0)
+  if (dtype == VQC_C64) {
+    if (write) VQC_PB(float, true); else VQC_PB(float, false);
+  } else {
+    if (write) VQC_PB(double, true); else VQC_PB(double, false);
+  }
+#undef VQC_PB
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+int serve_launch_pauli_reduce(const PauliRed* d_items, int nitems, cudaStream_t stream) {
+  if (nitems == 0) return VQC_OK;
+  k_pauli_reduce_batch<<<nitems, 32, 0, stream>>>(d_items);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+}  // namespace vqc

@@ -31,54 +31,9 @@
 
 #include "engine.h"
 #include "subspace.cuh"
+#include "tile_plan.cuh"
 
 namespace vqc {
-
-constexpr int kRegBits = 4;  // 16 amplitudes per thread
-constexpr int kMaxSlots = 64;
-constexpr int kMaxOpsPerPass = 192;  // bounds the pass's descriptors staged in shared memory
-enum { kOpU1 = 1, kOpU2 = 2, kOpDiag = 3, kOpAccD = 4 };
-
-struct DevPass {
-  uint64_t nontile_mask;  // global bits enumerated by the tile counter
-  int64_t ntiles;
-  int32_t stage_begin, stage_end;
-  int32_t nslots;
-  int32_t nops;           // ops of this pass (copied to shared memory with the stages)
-  int32_t npool;          // matrix pool entries of this pass
-  int32_t pad;
-};
-
-// Shared-memory bytes of one pass: tiles, accumulation slots, and the pass's
-// own stage / op / matrix descriptors (read by every thread for every op, so
-// they are staged once per CTA instead of being fetched through L1/L2).
-template <class R, int M, bool ADJ>
-__host__ __device__ constexpr size_t tile_bytes() {
-  return (size_t)(ADJ ? 2 : 1) * (size_t(1) << M) * sizeof(cplx<R>);
-}
-
-struct alignas(16) DevStage {
-  uint32_t dep[16];    // tile index of register slot j (OR with the thread part)
-  int64_t gdep[16];    // global offset of register slot j
-  uint64_t gthr_mask;  // global qubits of the thread's tile bits
-  uint32_t thr_mask;   // tile bits held by the thread index, ascending
-  int32_t op_begin, op_end, pad;
-};
-
-// code: bits 0-3 op type, 4-5 r0, 6-7 r1, 8 tile-bit controls, 9 non-tile
-// controls, 10 accumulate.  The first 16 bytes are read as one vector load.
-struct alignas(16) DevOp {
-  int32_t code;
-  int32_t mat;     // pool offset (complex elements)
-  uint32_t cmask, cval;  // controls on tile bits
-  uint64_t gmask, gval;  // controls on non-tile qubits
-  int32_t slot;    // accumulation slot or -1
-  int32_t nd;      // diagonal ops: number of qubits
-  int32_t dbit[5];  // tile bit of diagonal qubit i, or -1
-  int32_t dglob[5]; // global qubit of diagonal qubit i when not a tile bit
-};
-constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
-// bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries accumulated
 
 // ----------------------------------------------------------------------------- device helpers
 template <class R>
@@ -329,10 +284,10 @@ struct MinBlocks {
 };
 
 template <class R, int M, bool ADJ>
-__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
-    k_tile(cplx<R>* __restrict__ psi, cplx<R>* __restrict__ lam, const DevPass* __restrict__ pass,
-           const DevStage* __restrict__ stages, const DevOp* __restrict__ ops, const cplx<R>* __restrict__ pool,
-           double* __restrict__ partials) {
+__device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __restrict__ lam,
+                                          const DevPass* __restrict__ pass, const DevStage* __restrict__ stages,
+                                          const DevOp* __restrict__ ops, const cplx<R>* __restrict__ pool,
+                                          double* __restrict__ partials, int ncta) {
   constexpr int NT = 1 << (M - kRegBits), T = 1 << M, NW = NT / 32;
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -365,7 +320,7 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
   }
   C v[16], w[16];
   const int s_first = P.stage_begin, s_last = P.stage_end - 1;
-  for (int64_t tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
+  for (int64_t tile = blockIdx.x; tile < P.ntiles; tile += ncta) {
     const int64_t base = dep64(tile, P.nontile_mask);
     for (int s = s_first; s <= s_last; ++s) {
       const DevStage* S = stages + s;
@@ -482,6 +437,23 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
   }
 }
 
+// One pass of one state (the single-request path).
+template <class R, int M, bool ADJ>
+__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
+    k_tile(cplx<R>* psi, cplx<R>* lam, const DevPass* pass, const DevStage* stages, const DevOp* ops,
+           const cplx<R>* pool, double* partials) {
+  tile_body<R, M, ADJ>(psi, lam, pass, stages, ops, pool, partials, gridDim.x);
+}
+
+template <class R, int M, bool ADJ>
+__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
+    k_tile_batch(const TileItem* __restrict__ items) {
+  const TileItem it = items[blockIdx.y];
+  if ((int)blockIdx.x >= it.ncta) return;
+  tile_body<R, M, ADJ>((cplx<R>*)it.psi, (cplx<R>*)it.lam, it.pass, it.stages, it.ops, (const cplx<R>*)it.pool,
+                       it.partials, it.ncta);
+}
+
 // Sums the per-CTA partials over the grid in a fixed order: block = slot.
 __global__ void __launch_bounds__(256) k_reduce_slots(const double* __restrict__ partials, int nblocks, int nslots,
                                                       int row0, double* __restrict__ out) {
@@ -503,23 +475,6 @@ __global__ void __launch_bounds__(256) k_reduce_slots(const double* __restrict__
 }
 
 // ----------------------------------------------------------------------------- host planner
-struct PGrad {
-  int param;             // caller's parameter index
-  std::vector<cd> D;     // U1: 2x2 over the target (control subspace); AccD: 2^nd diagonal bins
-};
-
-struct FOp {
-  int kind = 0;          // kOpU1, kOpU2, kOpDiag, kOpAccD
-  int tq[2] = {-1, -1};  // target qubits (ascending)
-  uint64_t cmask = 0, cval = 0;  // control qubits and their firing values (global bits)
-  uint64_t qubits = 0;   // every qubit the op reads or writes
-  std::vector<cd> mat;   // U1 2x2, U2 4x4 (bit 0 <-> tq[0]), diagonal 2^nd table
-  int nd = 0;
-  int dq[5] = {0, 0, 0, 0, 0};
-  bool acc = false;
-  std::vector<PGrad> grads;
-};
-
 // A gate in planner form: one op, or "standalone" (kept as a GateSpec).
 struct PItem {
   bool standalone = false;
@@ -646,11 +601,14 @@ struct TileConfig {
   int clow;   // always-resident low qubits
 };
 
-static TileConfig tile_config(int dtype, bool adj) {
-  (void)adj;
-  if (dtype == VQC_C64) return {12, 4};
-  return {11, 3};
+static TileConfig tile_config(int dtype, int n) {
+  // 2^12 FP32 or 2^11 FP64 amplitudes per tile (32 KiB per state), smaller
+  // tiles for smaller states; the lowest 4 (FP32) / 3 (FP64) qubits are always
+  // tile qubits so that a tile is made of 128-byte runs
+  const int M = std::min(dtype == VQC_C64 ? 12 : 11, n);
+  return {M, std::min(dtype == VQC_C64 ? 4 : 3, M)};
 }
+constexpr int kMinTileBits = 9;  // 32 threads x 16 amplitudes
 
 // Greedy pass formation (see the file comment).  items are in execution order.
 static void plan_passes(int n, const TileConfig& tc, bool adj, std::vector<PItem>& items, std::vector<PlanPass>& out) {
@@ -829,10 +787,6 @@ struct Device {
   }
 };
 
-struct PassShape {
-  int nslots = 0, nstages = 0, nops = 0, npool = 0;
-};
-
 template <class R, int M, bool ADJ>
 static size_t pass_smem(const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
@@ -868,15 +822,6 @@ static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, con
 
 int standalone_adjoint(vqc_state h, void* lam, void* y, const GateSpec& gs, bool acc, double* out);
 
-// Runs a planned sequence of passes.  psi (and lam in ADJ mode) are device
-// buffers of h's size.  specs: the analysed gates (daggered in ADJ mode);
-// rows_out (ADJ): device rows of 8 doubles per accumulation, filled in pass
-// order; returns the list of (row, op) in `accs`.
-struct AccRef {
-  int row;
-  FOp op;
-};
-
 // The structure class of a one-qubit matrix (exact zeros: the matrices are
 // built from closed forms, so structural zeros are exact).
 static int u1_form(const std::vector<cd>& m) {
@@ -902,25 +847,20 @@ static int acc_kind(const FOp& f) {
 }
 
 template <class R, int M, bool ADJ>
-static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
-                    std::vector<AccRef>* accs, double* rows_dev) {
-  const int n = h->nq;
-  // serialise every pass into one device buffer
+static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, SerialPlan& sp, std::vector<AccRef>* accs) {
   Device d;
   std::vector<cplx<R>> pool;
-  struct Loc {
-    size_t pass, stages, ops;
-    size_t pool_begin;  // in pool entries, a multiple of 16 bytes
-    PassShape shape;
-    int nslots;
-    int row0;
-  };
-  std::vector<Loc> locs(passes.size());
+  std::vector<PassLoc>& locs = sp.locs;
+  locs.assign(passes.size(), PassLoc());
   int row = 0;
   for (size_t pi = 0; pi < passes.size(); ++pi) {
     PlanPass& p = passes[pi];
-    if (p.standalone) continue;
-    plan_stages(p, M, h->dtype);
+    if (p.standalone) {
+      locs[pi].standalone = true;
+      locs[pi].gate = p.gate;
+      continue;
+    }
+    plan_stages(p, M, dtype);
     std::vector<DevStage> ds;
     std::vector<DevOp> dops;
     std::map<int, int> tbit;
@@ -1012,6 +952,7 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     DevPass P{};
     P.nontile_mask = ((n >= 64) ? ~0ull : ((1ull << n) - 1)) & ~tile_mask;
     P.ntiles = int64_t(1) << (n - M);
+    locs[pi].ntiles = P.ntiles;
     P.nslots = slot;
     P.nops = (int)dops.size();
     P.npool = (int)(pool.size() - pool_begin);
@@ -1048,14 +989,45 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     prof_note("plan_standalone_gates", nsa);
   }
   for (int i = 0; i < 2; ++i) pool.push_back(mkc<R>(R(0), R(0)));  // the staging copy reads whole 16-byte words
-  const size_t pool_off = d.put(pool.data(), pool.size());
-  int rc = upload_ops(h, d.buf.data(), d.buf.size());
+  for (int i = 0; i < 2; ++i) pool.push_back(mkc<R>(R(0), R(0)));  // the staging copy reads whole 16-byte words
+  sp.pool_off = d.put(pool.data(), pool.size());
+  sp.rows = row;
+  sp.buf.swap(d.buf);
+}
+
+static void note_plan(bool adj, const std::vector<PlanPass>& passes) {
+  long long np = 0, ns = 0, no = 0, nsa = 0;
+  for (auto& p : passes) {
+    if (p.standalone) {
+      ++nsa;
+      continue;
+    }
+    ++np;
+    ns += (long long)p.stages.size();
+    no += (long long)p.ops.size();
+  }
+  prof_note(adj ? "plan_adjoint_passes" : "plan_forward_passes", np);
+  prof_note(adj ? "plan_adjoint_stages" : "plan_forward_stages", ns);
+  prof_note(adj ? "plan_adjoint_ops" : "plan_forward_ops", no);
+  prof_note("plan_standalone_gates", nsa);
+}
+
+template <class R, int M, bool ADJ>
+static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
+                    std::vector<AccRef>* accs, double* rows_dev) {
+  const int n = h->nq;
+  SerialPlan sp;
+  serialize_plan<R, M, ADJ>(n, h->dtype, passes, sp, accs);
+  note_plan(ADJ, passes);
+  const std::vector<PassLoc>& locs = sp.locs;
+  const size_t pool_off = sp.pool_off;
+  int rc = upload_ops(h, sp.buf.data(), sp.buf.size());
   if (rc) return rc;
   const unsigned char* base = (const unsigned char*)h->opbuf;
   // partial sums scratch: one row of 8 doubles per (CTA, slot) of the largest pass
   size_t need = 0;
   for (size_t pi = 0; pi < passes.size(); ++pi)
-    if (!passes[pi].standalone && locs[pi].nslots > 0)
+    if (!locs[pi].standalone && locs[pi].nslots > 0)
       need = std::max(need, (size_t)tile_grid<R, M, ADJ>(h->device, locs[pi].shape) * locs[pi].nslots * 8 *
                                 sizeof(double));
   double* partials = nullptr;
@@ -1072,9 +1044,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     partials = (double*)h->fused_scratch;
   }
   for (size_t pi = 0; pi < passes.size(); ++pi) {
-    PlanPass& p = passes[pi];
-    if (p.standalone) {
-      const GateSpec& gs = specs[p.gate];
+    if (locs[pi].standalone) {
+      const GateSpec& gs = specs[locs[pi].gate];
       if (ADJ) {
         if ((rc = standalone_adjoint(h, lam, psi, gs, false, nullptr))) return rc;
       } else {
@@ -1083,7 +1054,7 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
       continue;
     }
     const int nslots = locs[pi].nslots;
-    const int grid = tile_grid<R, M, ADJ>(h->device, locs[pi].shape);
+    const int grid = (int)std::min<int64_t>(tile_grid<R, M, ADJ>(h->device, locs[pi].shape), locs[pi].ntiles);
     if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, (const DevPass*)(base + locs[pi].pass),
                                       (const DevStage*)(base + locs[pi].stages), (const DevOp*)(base + locs[pi].ops),
                                       base + pool_off + locs[pi].pool_begin * sizeof(cplx<R>), partials, grid,
@@ -1097,10 +1068,7 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   return VQC_OK;
 }
 
-int fused_supported(vqc_state h) {
-  const TileConfig tc = tile_config(h->dtype, false);
-  return h->nq >= tc.M && h->nq <= 40;
-}
+int fused_supported(vqc_state h) { return h->nq >= kMinTileBits && h->nq <= 40; }
 
 template <class R, int M>
 static int forward_impl(vqc_state h, const vqc_gate* gates, int ngates, const double* mats) {
@@ -1113,7 +1081,7 @@ static int forward_impl(vqc_state h, const vqc_gate* gates, int ngates, const do
     items[i].standalone = !to_fop(specs[i], items[i].op);
   }
   std::vector<PlanPass> passes;
-  plan_passes(h->nq, tile_config(h->dtype, false), false, items, passes);
+  plan_passes(h->nq, tile_config(h->dtype, h->nq), false, items, passes);
   return run_plan<R, M, false>(h, h->d, nullptr, passes, specs, nullptr, nullptr);
 }
 
@@ -1125,23 +1093,27 @@ int apply_circuit_fused(vqc_state h, const vqc_gate* gates, int ngates, const do
     }
     return VQC_OK;
   }
-  return h->dtype == VQC_C64 ? forward_impl<float, 12>(h, gates, ngates, mats)
-                             : forward_impl<double, 11>(h, gates, ngates, mats);
+  switch (tile_config(h->dtype, h->nq).M + (h->dtype == VQC_C64 ? 0 : 100)) {
+    case 12: return forward_impl<float, 12>(h, gates, ngates, mats);
+    case 11: return forward_impl<float, 11>(h, gates, ngates, mats);
+    case 10: return forward_impl<float, 10>(h, gates, ngates, mats);
+    case 9: return forward_impl<float, 9>(h, gates, ngates, mats);
+    case 111: return forward_impl<double, 11>(h, gates, ngates, mats);
+    case 110: return forward_impl<double, 10>(h, gates, ngates, mats);
+    default: return forward_impl<double, 9>(h, gates, ngates, mats);
+  }
 }
 
 // Reverse sweep on the tile engine.  grads[j] receive the partials.  Gates
 // the tile engine cannot take (3+ targets, or 2 targets with parameters) run
 // through the per-gate adjoint path.
-struct ParamInfo {
-  int index;
-  std::vector<cd> D;  // U^dagger dU/dtheta, sorted order
-};
 int per_gate_params_grad(vqc_state h, void* lam, void* y, const GateSpec& gs, const std::vector<ParamInfo>& ps,
                          double* grads);
 
-template <class R, int M>
-static int reverse_impl(vqc_state h, void* lam, void* y, const std::vector<GateSpec>& specs,
-                        const std::vector<std::vector<ParamInfo>>& params, double* grads) {
+// The reverse sweep's op list: gates last to first (specs hold U^dagger),
+// with the reduced-matrix accumulation on every op that carries parameters.
+static std::vector<PItem> reverse_items(const std::vector<GateSpec>& specs,
+                                        const std::vector<std::vector<ParamInfo>>& params) {
   const int ng = (int)specs.size();
   std::vector<PItem> items;
   items.reserve(ng);
@@ -1170,8 +1142,15 @@ static int reverse_impl(vqc_state h, void* lam, void* y, const std::vector<GateS
     it.standalone = !ok;
     items.push_back(std::move(it));
   }
+  return items;
+}
+
+template <class R, int M>
+static int reverse_impl(vqc_state h, void* lam, void* y, const std::vector<GateSpec>& specs,
+                        const std::vector<std::vector<ParamInfo>>& params, double* grads) {
+  std::vector<PItem> items = reverse_items(specs, params);
   std::vector<PlanPass> passes;
-  plan_passes(h->nq, tile_config(h->dtype, true), true, items, passes);
+  plan_passes(h->nq, tile_config(h->dtype, h->nq), true, items, passes);
   // standalone gates with parameters: split their passes out so the per-gate
   // path can evaluate the partials right after the uncompute
   std::vector<AccRef> accs;
@@ -1227,26 +1206,169 @@ static int reverse_impl(vqc_state h, void* lam, void* y, const std::vector<GateS
   if (row_base > 0)
     VQC_CK(cudaMemcpyAsync(A.data(), h->accbuf, sizeof(double) * 8 * row_base, cudaMemcpyDeviceToHost, h->stream));
   VQC_CK(cudaStreamSynchronize(h->stream));
-  for (const AccRef& a : accs) {
-    const double* r = &A[(size_t)a.row * 8];
-    const cd Av[4] = {cd(r[0], r[1]), cd(r[2], r[3]), cd(r[4], r[5]), cd(r[6], r[7])};
-    for (const PGrad& pg : a.op.grads) {
-      double g = 0;
-      for (size_t i = 0; i < pg.D.size() && i < 4; ++i) {
-        // U1: D is 2x2 row-major and A[a][b] is stored at 2a+b; AccD: D is the
-        // diagonal bins and A's bins are stored in order
-        g += (pg.D[i] * Av[i]).real();
-      }
-      grads[pg.param] = g;
-    }
-  }
+  contract_grads(accs, A.data(), grads);
   return VQC_OK;
 }
 
 int reverse_sweep_fused(vqc_state h, void* lam, void* y, const std::vector<GateSpec>& specs,
                         const std::vector<std::vector<ParamInfo>>& params, double* grads) {
-  return h->dtype == VQC_C64 ? reverse_impl<float, 12>(h, lam, y, specs, params, grads)
-                             : reverse_impl<double, 11>(h, lam, y, specs, params, grads);
+  switch (tile_config(h->dtype, h->nq).M + (h->dtype == VQC_C64 ? 0 : 100)) {
+    case 12: return reverse_impl<float, 12>(h, lam, y, specs, params, grads);
+    case 11: return reverse_impl<float, 11>(h, lam, y, specs, params, grads);
+    case 10: return reverse_impl<float, 10>(h, lam, y, specs, params, grads);
+    case 9: return reverse_impl<float, 9>(h, lam, y, specs, params, grads);
+    case 111: return reverse_impl<double, 11>(h, lam, y, specs, params, grads);
+    case 110: return reverse_impl<double, 10>(h, lam, y, specs, params, grads);
+    default: return reverse_impl<double, 9>(h, lam, y, specs, params, grads);
+  }
+}
+
+}  // namespace vqc
+
+namespace vqc {
+
+// g_j = Re sum_ab D_j[a][b] A[a][b] for every parameter of every accumulating op
+// (U1: D is 2x2 row-major and A[a][b] sits at 2a+b; AccD: diagonal bins in order).
+void contract_grads(const std::vector<AccRef>& accs, const double* A, double* grads) {
+  for (const AccRef& a : accs) {
+    const double* r = &A[(size_t)a.row * 8];
+    const cd Av[4] = {cd(r[0], r[1]), cd(r[2], r[3]), cd(r[4], r[5]), cd(r[6], r[7])};
+    for (const PGrad& pg : a.op.grads) {
+      double g = 0;
+      for (size_t i = 0; i < pg.D.size() && i < 4; ++i) g += (pg.D[i] * Av[i]).real();
+      grads[pg.param] = g;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------- serving support
+__global__ void __launch_bounds__(256) k_reduce_slots_batch(const RedItem* __restrict__ items) {
+  __shared__ double sm[8][8];
+  const RedItem it = items[blockIdx.y];
+  const int slot = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (slot >= it.nslots) return;
+  for (int val = 0; val < 8; ++val) {
+    double s = 0;
+    for (int b = threadIdx.x; b < it.nblocks; b += blockDim.x)
+      s += it.partials[((size_t)b * it.nslots + slot) * 8 + val];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) sm[warp][val] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    double s = 0;
+    for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) s += sm[wp][threadIdx.x];
+    it.out[(size_t)slot * 8 + threadIdx.x] = s;
+  }
+}
+
+template <class R, int M>
+static int build_plan_tm(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
+                         const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp) {
+  const TileConfig tc = tile_config(dtype, n);
+  auto shape_max = [](const SerialPlan& sp) {
+    PassShape m;
+    for (const PassLoc& l : sp.locs) {
+      m.nslots = std::max(m.nslots, l.shape.nslots);
+      m.nstages = std::max(m.nstages, l.shape.nstages);
+      m.nops = std::max(m.nops, l.shape.nops);
+      m.npool = std::max(m.npool, l.shape.npool);
+    }
+    return m;
+  };
+  std::vector<PItem> items(fspecs.size());
+  for (size_t i = 0; i < fspecs.size(); ++i) {
+    items[i].gate = (int)i;
+    items[i].standalone = !to_fop(fspecs[i], items[i].op);
+  }
+  std::vector<PlanPass> passes;
+  plan_passes(n, tc, false, items, passes);
+  for (const PlanPass& p : passes)
+    if (p.standalone) return fail(VQC_ERR_UNSUPPORTED, "serving takes gates with at most two target qubits");
+  serialize_plan<R, M, false>(n, dtype, passes, rp.fwd, nullptr);
+  rp.fwd_max = shape_max(rp.fwd);
+  if (want_grad) {
+    std::vector<PItem> ritems = reverse_items(rspecs, params);
+    std::vector<PlanPass> rpasses;
+    plan_passes(n, tc, true, ritems, rpasses);
+    for (const PlanPass& p : rpasses)
+      if (p.standalone)
+        return fail(VQC_ERR_UNSUPPORTED, "serving takes parameterised gates with one target qubit (or diagonal)");
+    serialize_plan<R, M, true>(n, dtype, rpasses, rp.adj, &rp.accs);
+    rp.adj_max = shape_max(rp.adj);
+  }
+  rp.M = M;
+  rp.ntiles = int64_t(1) << (n - M);
+  return VQC_OK;
+}
+
+int serve_build_plan(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
+                     const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp) {
+  if (n < kMinTileBits || n > 40) return fail(VQC_ERR_UNSUPPORTED, "serving takes 9 to 40 qubits");
+  switch (tile_config(dtype, n).M + (dtype == VQC_C64 ? 0 : 100)) {
+    case 12: return build_plan_tm<float, 12>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+    case 11: return build_plan_tm<float, 11>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+    case 10: return build_plan_tm<float, 10>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+    case 9: return build_plan_tm<float, 9>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+    case 111: return build_plan_tm<double, 11>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+    case 110: return build_plan_tm<double, 10>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+    default: return build_plan_tm<double, 9>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+  }
+}
+
+template <class R, int M, bool ADJ>
+static int grid_x_tm(const PassShape& maxs, int64_t max_ntiles, int device) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>(max_ntiles, tile_grid<R, M, ADJ>(device, maxs)));
+}
+
+template <class R, int M, bool ADJ>
+static int launch_batch_tm(const TileItem* d_items, int nitems, int gridx, const PassShape& maxs,
+                           cudaStream_t stream) {
+  constexpr int NT = 1 << (M - kRegBits);
+  const size_t smem = pass_smem<R, M, ADJ>(maxs);
+  auto kfun = k_tile_batch<R, M, ADJ>;
+  VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
+  ProfScope prof(stream, ADJ ? "serve_tile_adjoint" : "serve_tile_forward", 0);
+  kfun<<<dim3(gridx, nitems), NT, smem, stream>>>(d_items);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+
+#define VQC_TILE_SWITCH(FN, ...)                                         \
+  switch (M + (dtype == VQC_C64 ? 0 : 100) + (adj ? 1000 : 0)) {          \
+    case 12: return FN<float, 12, false>(__VA_ARGS__);                    \
+    case 11: return FN<float, 11, false>(__VA_ARGS__);                    \
+    case 10: return FN<float, 10, false>(__VA_ARGS__);                    \
+    case 9: return FN<float, 9, false>(__VA_ARGS__);                      \
+    case 1012: return FN<float, 12, true>(__VA_ARGS__);                   \
+    case 1011: return FN<float, 11, true>(__VA_ARGS__);                   \
+    case 1010: return FN<float, 10, true>(__VA_ARGS__);                   \
+    case 1009: return FN<float, 9, true>(__VA_ARGS__);                    \
+    case 111: return FN<double, 11, false>(__VA_ARGS__);                  \
+    case 110: return FN<double, 10, false>(__VA_ARGS__);                  \
+    case 109: return FN<double, 9, false>(__VA_ARGS__);                   \
+    case 1111: return FN<double, 11, true>(__VA_ARGS__);                  \
+    case 1110: return FN<double, 10, true>(__VA_ARGS__);                  \
+    case 1109: return FN<double, 9, true>(__VA_ARGS__);                   \
+    default: return fail(VQC_ERR_ARG, "no tile kernel for this size");   \
+  }
+
+int serve_tile_gridx(int dtype, int M, bool adj, const PassShape& maxs, int64_t max_ntiles, int device) {
+  VQC_TILE_SWITCH(grid_x_tm, maxs, max_ntiles, device)
+}
+
+int serve_launch_tiles(int dtype, int M, bool adj, const TileItem* d_items, int nitems, int gridx,
+                       const PassShape& maxs, cudaStream_t stream) {
+  VQC_TILE_SWITCH(launch_batch_tm, d_items, nitems, gridx, maxs, stream)
+}
+#undef VQC_TILE_SWITCH
+
+int serve_launch_reduce(const RedItem* d_items, int nitems, int maxslots, cudaStream_t stream) {
+  if (nitems == 0 || maxslots == 0) return VQC_OK;
+  k_reduce_slots_batch<<<dim3(maxslots, nitems), 256, 0, stream>>>(d_items);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
 }
 
 }  // namespace vqc

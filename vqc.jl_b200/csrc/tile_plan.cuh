@@ -1,0 +1,183 @@
+// Data structures of the tile engine shared by the single-state path
+// (fused.cu) and the serving loop (serve.cu): the device descriptors of a
+// pass, the planner's op form, and a serialised plan.
+#pragma once
+
+#include <vector>
+
+#include "engine.h"
+
+namespace vqc {
+
+constexpr int kRegBits = 4;  // 16 amplitudes per thread
+constexpr int kMaxSlots = 64;
+constexpr int kMaxOpsPerPass = 192;  // bounds the pass's descriptors staged in shared memory
+enum { kOpU1 = 1, kOpU2 = 2, kOpDiag = 3, kOpAccD = 4 };
+
+struct DevPass {
+  uint64_t nontile_mask;  // global bits enumerated by the tile counter
+  int64_t ntiles;
+  int32_t stage_begin, stage_end;
+  int32_t nslots;
+  int32_t nops;           // ops of this pass (copied to shared memory with the stages)
+  int32_t npool;          // matrix pool entries of this pass
+  int32_t pad;
+};
+
+// Shared-memory bytes of one pass: tiles, accumulation slots, and the pass's
+// own stage / op / matrix descriptors (read by every thread for every op, so
+// they are staged once per CTA instead of being fetched through L1/L2).
+template <class R, int M, bool ADJ>
+__host__ __device__ constexpr size_t tile_bytes() {
+  return (size_t)(ADJ ? 2 : 1) * (size_t(1) << M) * sizeof(cplx<R>);
+}
+
+struct alignas(16) DevStage {
+  uint32_t dep[16];    // tile index of register slot j (OR with the thread part)
+  int64_t gdep[16];    // global offset of register slot j
+  uint64_t gthr_mask;  // global qubits of the thread's tile bits
+  uint32_t thr_mask;   // tile bits held by the thread index, ascending
+  int32_t op_begin, op_end, pad;
+};
+
+// code: bits 0-3 op type, 4-5 r0, 6-7 r1, 8 tile-bit controls, 9 non-tile
+// controls, 10 accumulate.  The first 16 bytes are read as one vector load.
+struct alignas(16) DevOp {
+  int32_t code;
+  int32_t mat;     // pool offset (complex elements)
+  uint32_t cmask, cval;  // controls on tile bits
+  uint64_t gmask, gval;  // controls on non-tile qubits
+  int32_t slot;    // accumulation slot or -1
+  int32_t nd;      // diagonal ops: number of qubits
+  int32_t dbit[5];  // tile bit of diagonal qubit i, or -1
+  int32_t dglob[5]; // global qubit of diagonal qubit i when not a tile bit
+};
+constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
+// bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries accumulated
+
+// One pass each of many states in one launch (the serving path): request
+// blockIdx.y, its tiles strided over its own `ncta` CTAs (fixed per request,
+// so its sums are grouped the same way whatever it is batched with); CTAs
+// beyond ncta leave at once.
+struct TileItem {
+  void* psi;
+  void* lam;
+  const DevPass* pass;
+  const DevStage* stages;
+  const DevOp* ops;
+  const void* pool;
+  double* partials;  // [ncta][nslots][8]
+  int64_t ntiles;
+  int ncta;
+  int pad;
+};
+
+struct PGrad {
+  int param;             // caller's parameter index
+  std::vector<cd> D;     // U1: 2x2 over the target (control subspace); AccD: 2^nd diagonal bins
+};
+
+struct FOp {
+  int kind = 0;          // kOpU1, kOpU2, kOpDiag, kOpAccD
+  int tq[2] = {-1, -1};  // target qubits (ascending)
+  uint64_t cmask = 0, cval = 0;  // control qubits and their firing values (global bits)
+  uint64_t qubits = 0;   // every qubit the op reads or writes
+  std::vector<cd> mat;   // U1 2x2, U2 4x4 (bit 0 <-> tq[0]), diagonal 2^nd table
+  int nd = 0;
+  int dq[5] = {0, 0, 0, 0, 0};
+  bool acc = false;
+  std::vector<PGrad> grads;
+};
+
+struct PassShape {
+  int nslots = 0, nstages = 0, nops = 0, npool = 0;
+};
+
+// An accumulating op of the reverse sweep and the row of 8 doubles (the
+// reduced matrix A) its partial sums land in.
+struct AccRef {
+  int row;
+  FOp op;
+};
+
+struct PassLoc {
+  bool standalone = false;
+  int gate = -1;
+  size_t pass = 0, stages = 0, ops = 0;
+  size_t pool_begin = 0;  // in pool entries, a multiple of 16 bytes
+  PassShape shape;
+  int nslots = 0;
+  int row0 = 0;
+  int64_t ntiles = 0;
+};
+
+// A plan serialised for the device: one byte image holding every pass's
+// DevPass, stages and ops, then the matrix pool; offsets in `locs`.
+struct SerialPlan {
+  std::vector<unsigned char> buf;
+  std::vector<PassLoc> locs;
+  size_t pool_off = 0;
+  int rows = 0;  // accumulation rows (ADJ)
+};
+
+
+// Pauli-sum tables (expect.cu): terms grouped by flip mask x.
+struct DevTerm {
+  uint64_t z;
+  double2 c;  // coefficient for the expectation, times i^{popcount(x & z)}
+  double2 d;  // coefficient for the applied operator, same phase
+};
+struct DevGroup {
+  uint64_t x;
+  int start, count;
+};
+
+// One state's Pauli pass in a batched launch (serving path).
+struct PauliItem {
+  const void* ket;  // the state (also the bra: <psi|H|psi>)
+  void* out;        // (H + H^dagger) psi for gradient requests, else unused
+  int64_t N;
+  const DevGroup* groups;
+  int ng;
+  const DevTerm* terms;
+  int nt;
+  double* partials;  // [gridDim.x][2]
+};
+struct PauliRed {
+  const double* partials;
+  int nblocks;
+  double* out;  // energy (re, im)
+};
+int serve_pauli_image(int nq, const vqc_pauli* terms, int nterms, bool hermitian_part, std::vector<unsigned char>& img,
+                      int& ng, int& nt);
+int serve_launch_pauli(int dtype, bool write, const PauliItem* d_items, int nitems, int gridx, size_t smem,
+                       cudaStream_t stream);
+int serve_launch_pauli_reduce(const PauliRed* d_items, int nitems, cudaStream_t stream);
+
+// Reduction of one request's per-CTA accumulation partials (serving path).
+struct RedItem {
+  const double* partials;  // [nblocks][nslots][8]
+  int nblocks;
+  int nslots;
+  double* out;  // [nslots][8]
+};
+
+// A request's plan for the serving loop: forward passes, and for gradient
+// requests the reverse passes and their accumulation rows.
+struct ReqPlan {
+  int M = 0;
+  SerialPlan fwd, adj;
+  std::vector<AccRef> accs;
+  PassShape fwd_max, adj_max;
+  int64_t ntiles = 0;
+};
+
+int serve_build_plan(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
+                     const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp);
+int serve_tile_gridx(int dtype, int M, bool adj, const PassShape& maxs, int64_t max_ntiles, int device);
+int serve_launch_tiles(int dtype, int M, bool adj, const TileItem* d_items, int nitems, int gridx,
+                       const PassShape& maxs, cudaStream_t stream);
+int serve_launch_reduce(const RedItem* d_items, int nitems, int maxslots, cudaStream_t stream);
+void contract_grads(const std::vector<AccRef>& accs, const double* A, double* grads);
+
+}  // namespace vqc
