@@ -438,6 +438,108 @@ def run_dm_n13(args, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def run_serve(args, local_rank):
+    """Serving stream (continuous batching): requests with n ~ U{10..22},
+    depth ~ U{2..12} layers of the hardware-efficient ansatz (RY, RZ on every
+    qubit + CNOT ladder), angles ~ U[0, 2 pi), half energy only and half energy
+    + gradient, transverse-field Ising H with g ~ U[0.2, 1.5]; Poisson arrivals
+    at swept rates.  FP32 states, FP64 accumulation.  Baseline: one request at
+    a time through the plain FP64 single-request path, same arrival sequence."""
+    import threading
+
+    import torch
+    import vqcb200 as V
+    from vqcb200 import workloads as W
+    from vqcb200.circuit import Packed
+    from vqcb200.serve import Server
+    torch.cuda.set_device(local_rank)
+    V.load()
+    rng = np.random.default_rng(SEED)
+    nreq = args.requests
+    reqs = []
+    for i in range(nreq):
+        n = int(rng.integers(10, 23))
+        layers = int(rng.integers(2, 13))
+        th = rng.uniform(0, 2 * np.pi, layers * 2 * n)
+        g = float(rng.uniform(0.2, 1.5))
+        want = bool(rng.integers(0, 2))
+        c = W.to_circuit(W.hea_spec(n, layers, th))
+        H = W.to_operator(W.tfim_spec(n, g))
+        arr, nt = H.packed()
+        reqs.append((n, Packed(c, with_params=want), arr, nt, want, c, H))
+
+    def stream(rate, count):
+        """Submit `count` requests with Poisson arrivals at `rate`/s; latencies in s."""
+        arrivals = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, count))
+        lat = [None] * count
+        with Server(device=local_rank, dtype=np.complex64, memory_bytes=args.serve_memory << 20,
+                    max_active=args.serve_slots, planner_threads=4) as srv:
+            tickets = [None] * count
+            done = threading.Event()
+
+            def collector():
+                for i in range(count):
+                    while tickets[i] is None:
+                        time.sleep(0.0002)
+                    e, gr, l = srv.wait(tickets[i], timeout=600)
+                    lat[i] = l
+                done.set()
+            th = threading.Thread(target=collector)
+            th.start()
+            t0 = time.perf_counter()
+            for i in range(count):
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                n, p, arr, nt, want = reqs[i % nreq][:5]
+                tickets[i] = srv.submit_packed(n, p, arr, nt, want)
+            done.wait()
+            makespan = time.perf_counter() - t0
+            th.join()
+            st = srv.stats()
+            tm = srv.timing()
+        lat = np.array(lat)
+        return {"rate_offered": rate, "requests": count, "throughput": count / makespan,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "mean_batch": st["request_steps"] / max(st["launches"], 1), "loop_iterations": st["iterations"],
+                "phases_ms": {k: round(v * 1e3, 3) for k, v in tm.items()}}
+
+    # baseline: plain FP64, one request at a time, in arrival order
+    def baseline(rate, count):
+        arrivals = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, count))
+        lat = []
+        t0 = time.perf_counter()
+        for i in range(count):
+            dt = arrivals[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            n, p, arr, nt, want, c, H = reqs[i % nreq]
+            psi0 = V.StateVector(n, dtype=np.complex128, device=local_rank)
+            if want:
+                V.energy_and_gradient(H, c, psi0)
+            else:
+                V.expectation(H, c * psi0)
+            lat.append(time.perf_counter() - t0 - arrivals[i])
+        makespan = time.perf_counter() - t0
+        lat = np.array(lat)
+        return {"rate_offered": rate, "requests": count, "throughput": count / makespan,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}
+
+    # warm-up (kernel loads, allocator pools)
+    stream(200.0, min(200, nreq))
+    rates = [float(r) for r in args.rates.split(",")]
+    results = [stream(r, nreq) for r in rates]
+    # service rate of the one-at-a-time baseline: back-to-back requests
+    base_sat = baseline(1e6, min(args.baseline_requests, nreq))
+    base = [baseline(r, min(args.baseline_requests, nreq)) for r in rates if r < 0.9 * base_sat["throughput"]]
+    out = {"metric": "serving throughput and p50/p99 latency (continuous batching, FP32 states)", "unit": "requests/s",
+           "config": {"workload": "n~U{10..22}, 2..12 HEA layers, 50% energy / 50% energy+gradient, TFIM g~U[0.2,1.5], "
+                                  "Poisson arrivals", "requests_per_rate": nreq, "memory_budget_MiB": args.serve_memory,
+                      "slots": args.serve_slots},
+           "served": results, "baseline_fp64_one_at_a_time": {"saturated": base_sat, "at_rates": base}}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -447,7 +549,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
-    ap.add_argument("--workload", default="adjoint", choices=["adjoint", "gates_n30", "dm_n13"],
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests per rate")
+    ap.add_argument("--rates", default="500,1000,2000,4000", help="serve: offered rates (requests/s)")
+    ap.add_argument("--baseline-requests", type=int, default=200, help="serve: requests of the FP64 baseline")
+    ap.add_argument("--serve-memory", type=int, default=16384, help="serve: device memory budget (MiB)")
+    ap.add_argument("--serve-slots", type=int, default=512, help="serve: requests in flight at most")
+    ap.add_argument("--workload", default="adjoint", choices=["adjoint", "gates_n30", "dm_n13", "serve"],
                     help="adjoint (the headline) or a secondary workload")
     ap.add_argument("--qubits", type=int, default=None,
                     help="state size (default 26, the headline; smaller sizes are for profiling captures)")
@@ -466,6 +573,9 @@ def main():
         return
     if args.workload == "dm_n13":
         run_dm_n13(args, local_rank)
+        return
+    if args.workload == "serve":
+        run_serve(args, local_rank)
         return
     if world > 1:
         import datetime

@@ -205,6 +205,9 @@ int vqc_serve_wait(vqc_server s, int64_t ticket, int timeout_ms, double* energy,
 /* out[0..6]: completed, loop iterations, launches, request-steps launched,
  * device bytes admitted, requests running, requests waiting. */
 int vqc_serve_stats(vqc_server s, long long* out);
+/* out[0..5] (seconds): mean and max planning time, mean and max wait for
+ * admission, mean and max time from admission to completion. */
+int vqc_serve_timing(vqc_server s, double* out);
 int vqc_serve_close(vqc_server s);
 
 #ifdef __cplusplus

@@ -79,7 +79,7 @@ struct Request {
   int status = 0;  // 0 queued, 1 planned, 2 running, 3 done, < 0 error
   std::string error;
   double energy[2] = {0, 0};
-  double t_submit = 0, t_done = 0;
+  double t_submit = 0, t_planned = 0, t_admit = 0, t_done = 0;
   int nfwd() const { return (int)plan.fwd.locs.size(); }
   int nadj() const { return grad ? (int)plan.adj.locs.size() : 0; }
   int nsteps() const { return nfwd() + 1 + nadj(); }
@@ -110,6 +110,7 @@ struct vqc_server_s {
   size_t items_cap = 0;
   // statistics
   long long completed = 0, iterations = 0, launches = 0, items_launched = 0;
+  double plan_s_max = 0, wait_s_max = 0, run_s_max = 0, plan_s_sum = 0, wait_s_sum = 0, run_s_sum = 0;
   std::string fatal;
 };
 
@@ -196,6 +197,7 @@ static void planner_main(vqc_server_s* s) {
       s->cv_done.notify_all();
     } else {
       r->status = 1;
+      r->t_planned = now_s();
       s->ready.push_back(r);
       s->cv_ready.notify_all();
     }
@@ -242,6 +244,7 @@ static void worker_main(vqc_server_s* s) {
         s->ready.pop_front();
         s->in_use += r->dbytes;
         r->status = 2;
+        r->t_admit = now_s();
         admitted.push_back(r);
       }
     }
@@ -490,6 +493,13 @@ static void worker_main(vqc_server_s* s) {
         r->status = 3;
         r->t_done = now_s();
         ++s->completed;
+        const double pl = r->t_planned - r->t_submit, wt = r->t_admit - r->t_planned, rn = r->t_done - r->t_admit;
+        s->plan_s_sum += pl;
+        s->wait_s_sum += wt;
+        s->run_s_sum += rn;
+        s->plan_s_max = std::max(s->plan_s_max, pl);
+        s->wait_s_max = std::max(s->wait_s_max, wt);
+        s->run_s_max = std::max(s->run_s_max, rn);
         s->cv_done.notify_all();
       } else {
         ++r->step;
@@ -530,6 +540,15 @@ int vqc_serve_open(int device, int dtype, size_t memory_bytes, int max_active, i
       (e = cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming)) != cudaSuccess) {
     delete s;
     return cuda_fail(e, "serving stream");
+  }
+  {
+    // keep freed request memory in the stream-ordered pool instead of
+    // returning it to the driver at every synchronisation
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
   }
   const int np = std::max(1, std::min(planner_threads, 16));
   for (int i = 0; i < np; ++i) s->planners.emplace_back(planner_main, s);
@@ -623,6 +642,19 @@ int vqc_serve_stats(vqc_server s, long long* out) {
   out[4] = (long long)s->in_use;
   out[5] = (long long)s->active.size();
   out[6] = (long long)s->ready.size() + (long long)s->to_plan.size();
+  return VQC_OK;
+}
+
+int vqc_serve_timing(vqc_server s, double* out) {
+  if (!s || !out) return fail(VQC_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  const double n = (double)std::max<long long>(s->completed, 1);
+  out[0] = s->plan_s_sum / n;
+  out[1] = s->plan_s_max;
+  out[2] = s->wait_s_sum / n;
+  out[3] = s->wait_s_max;
+  out[4] = s->run_s_sum / n;
+  out[5] = s->run_s_max;
   return VQC_OK;
 }
 

@@ -53,6 +53,19 @@ class Server:
         t.nparams = p.nparams
         return t
 
+    def submit_packed(self, nqubits, packed, terms, nterms, want_grad=True):
+        """submit() with a circuit already packed (vqcb200.circuit.Packed) and a
+        Pauli array (QubitsOperator.packed()); the objects must outlive the ticket."""
+        grads = np.zeros(max(packed.nparams, 1))
+        tid = ctypes.c_int64()
+        _lib.check(self._lib.vqc_serve_submit(self._h, nqubits, packed.gates, packed.ngates, packed.mats_ptr(),
+                                              packed.params, packed.nparams if want_grad else 0, terms, nterms,
+                                              1 if want_grad else 0, grads.ctypes.data_as(_lib._D),
+                                              ctypes.byref(tid)))
+        t = Ticket(tid.value, packed, terms, grads, want_grad)
+        t.nparams = packed.nparams
+        return t
+
     def _finish(self, t, e, lat):
         t.energy = complex(e[0], e[1])
         t.latency = lat.value
@@ -77,6 +90,12 @@ class Server:
         out = (ctypes.c_longlong * 7)()
         _lib.check(self._lib.vqc_serve_stats(self._h, out))
         keys = ["completed", "iterations", "launches", "request_steps", "bytes_admitted", "running", "waiting"]
+        return dict(zip(keys, list(out)))
+
+    def timing(self):
+        out = (ctypes.c_double * 6)()
+        _lib.check(self._lib.vqc_serve_timing(self._h, out))
+        keys = ["plan_mean_s", "plan_max_s", "wait_mean_s", "wait_max_s", "run_mean_s", "run_max_s"]
         return dict(zip(keys, list(out)))
 
     def close(self):
