@@ -177,6 +177,22 @@ int vqc_dm_probs(vqc_state rho, double* out);
 /* tr(rho) (densitymatrix.jl:58), FP64 (re, im). */
 int vqc_dm_trace(vqc_state rho, double* out);
 
+/* ---- allocation-free expectation (no counterpart in the reference) ------
+ * For callers that cannot allocate device memory (a fixed arena handed over
+ * at start-up, no cudaMalloc/cudaFree afterwards): expectation(H, psi) of a
+ * state in the caller's own device buffer `state` (2^nqubits amplitudes of
+ * `dtype`, on the current device), on `stream` (a cudaStream_t, or NULL for
+ * the default stream); out = (re, im) in FP64, the same quantity as
+ * vqc_expect_pauli.  All scratch lives in one static device array of the
+ * library (218,112 bytes per GPU that loads the library, held until exit);
+ * at most 1024 Pauli terms per call (more: VQC_ERR_ARG).  The first call on a
+ * device looks up the array's device address; make that first call before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * Blocks until the result is on the host. */
+int vqc_expect_pauli_noalloc(const void* state, int nqubits, int dtype, const vqc_pauli* terms, int nterms,
+                             void* stream, double* out);
+
 /* ---- serving: continuous batching of many circuits on one GPU (no
  *      counterpart in the reference, which evaluates one circuit per call) ----
  * A server owns one GPU stream, a worker thread and `planner_threads`

@@ -474,3 +474,115 @@ int serve_launch_pauli_reduce(const PauliRed* d_items, int nitems, cudaStream_t 
 }
 
 }  // namespace vqc
+
+// ----------------------------------------------------------------------------- allocation-free expectation
+// Some callers of this library cannot allocate device memory: a host
+// application that hands over a pre-sized arena and forbids cudaMalloc/cudaFree
+// after start-up (allocation there can stall other streams, fail under memory
+// pressure, or break a fixed memory plan), or code that must not touch the
+// allocator while other work is in flight.  For them, ⟨psi|H|psi⟩ of a state in
+// the caller's own device buffer runs here with all of its scratch (the Pauli
+// tables, the per-block partial sums, the last-block counter and the result)
+// in one static device array.  Every GPU that loads the library holds this
+// array until the process exits.
+namespace vqc {
+
+constexpr int kNoAllocMaxTerms = 1024;    // Pauli terms per call at most
+constexpr int kNoAllocMaxBlocks = 296;    // reduction grid at most
+constexpr size_t kNoAllocTableBytes = kNoAllocMaxTerms * (sizeof(DevTerm) + sizeof(DevGroup));
+constexpr size_t kNoAllocPartialBytes = (size_t)kNoAllocMaxBlocks * kMaxAcc * sizeof(double);
+constexpr size_t kNoAllocBytes = kNoAllocTableBytes + kNoAllocPartialBytes + 1024;  // + counter and result
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of the static scratch array, looked up once per device with
+// that device current (the array's name is only a host-side stand-in).
+static unsigned char* noalloc_scratch_ptr(int device) {
+  static std::mutex mu;
+  static unsigned char* ptrs[64] = {nullptr};
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!ptrs[device]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
+    ptrs[device] = (unsigned char*)p;
+  }
+  return ptrs[device];
+}
+
+}  // namespace vqc
+
+extern "C" int vqc_expect_pauli_noalloc(const void* state, int nqubits, int dtype, const vqc_pauli* terms,
+                                        int nterms, void* stream, double* out) {
+  using namespace vqc;
+  if (!state || !out) return fail(VQC_ERR_ARG, "null state or output");
+  if (dtype != VQC_C64 && dtype != VQC_C128) return fail(VQC_ERR_ARG, "dtype must be VQC_C64 or VQC_C128");
+  if (nqubits < 1 || nqubits > 40) return fail(VQC_ERR_ARG, "number of qubits must be in 1..40");
+  if (nterms < 0 || (nterms > 0 && !terms)) return fail(VQC_ERR_ARG, "bad Pauli term array");
+  if (nterms > kNoAllocMaxTerms)
+    return fail(VQC_ERR_ARG, "the allocation-free expectation takes at most 1024 Pauli terms per call");
+  int device = 0;
+  VQC_CK(cudaGetDevice(&device));
+  unsigned char* base = noalloc_scratch_ptr(device);
+  if (!base) return fail(VQC_ERR_CUDA, "cudaGetSymbolAddress of the static scratch array failed");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nterms == 0) {
+    out[0] = out[1] = 0;
+    return VQC_OK;
+  }
+  // group the terms by flip mask into a fixed-size table (no heap use)
+  const uint64_t lim = nqubits >= 64 ? ~0ull : ((1ull << nqubits) - 1);
+  int order[kNoAllocMaxTerms];
+  for (int i = 0; i < nterms; ++i) {
+    if ((terms[i].xmask & ~lim) || (terms[i].zmask & ~lim)) return fail(VQC_ERR_ARG, "Pauli term acts outside the register");
+    int j = i;
+    for (; j > 0 && terms[order[j - 1]].xmask > terms[i].xmask; --j) order[j] = order[j - 1];
+    order[j] = i;
+  }
+  // [groups][terms]: the terms are first written after room for nterms groups,
+  // then moved down behind the ng groups actually used
+  alignas(16) unsigned char table[kNoAllocTableBytes];
+  DevGroup* groups = reinterpret_cast<DevGroup*>(table);
+  DevTerm* dt = reinterpret_cast<DevTerm*>(table + sizeof(DevGroup) * nterms);
+  int ng = 0;
+  for (int a = 0; a < nterms; ++a) {
+    const vqc_pauli& t = terms[order[a]];
+    if (ng == 0 || groups[ng - 1].x != t.xmask) groups[ng++] = DevGroup{t.xmask, a, 0};
+    ++groups[ng - 1].count;
+    const int ny = __builtin_popcountll(t.xmask & t.zmask) & 3;
+    const cd ph[4] = {cd(1, 0), cd(0, 1), cd(-1, 0), cd(0, -1)};
+    const cd c = cd(t.coeff_re, t.coeff_im) * ph[ny];
+    dt[a] = DevTerm{t.zmask, make_double2(c.real(), c.imag()), make_double2(c.real(), c.imag())};
+  }
+  const size_t gb = sizeof(DevGroup) * ng, tb = sizeof(DevTerm) * nterms;
+  std::memmove(table + gb, dt, tb);
+  unsigned char* d_table = base;
+  Scratch scr;
+  scr.partials = reinterpret_cast<double*>(base + kNoAllocTableBytes);
+  scr.counter = reinterpret_cast<unsigned*>(base + kNoAllocTableBytes + kNoAllocPartialBytes);
+  scr.result = reinterpret_cast<double*>(base + kNoAllocTableBytes + kNoAllocPartialBytes + 256);
+  scr.max_blocks = kNoAllocMaxBlocks;
+  // the table (pageable source: staged before the call returns) and a zero counter
+  VQC_CK(cudaMemcpyAsync(d_table, table, gb + tb, cudaMemcpyHostToDevice, st));
+  VQC_CK(cudaMemsetAsync(scr.counter, 0, sizeof(unsigned), st));
+  const int64_t N = int64_t(1) << nqubits;
+  const int grid = std::min(reduction_grid(device, N), kNoAllocMaxBlocks);
+  const size_t smem = gb + tb;
+#define VQC_NOALLOC_LAUNCH(R)                                                                                    \
+  do {                                                                                                           \
+    auto kfun = k_pauli<R, false, true>;                                                                         \
+    if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kfun<<<grid, kRedThreads, smem, st>>>((const cplx<R>*)state, (const cplx<R>*)state, nullptr, N,              \
+                                          (const DevGroup*)d_table, ng, (const DevTerm*)(d_table + gb), nterms, scr, \
+                                          scr.result);                                                           \
+  } while (0)
+  if (dtype == VQC_C64)
+    VQC_NOALLOC_LAUNCH(float);
+  else
+    VQC_NOALLOC_LAUNCH(double);
+#undef VQC_NOALLOC_LAUNCH
+  VQC_CK(cudaGetLastError());
+  VQC_CK(cudaMemcpyAsync(out, scr.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  VQC_CK(cudaStreamSynchronize(st));
+  return VQC_OK;
+}
