@@ -198,7 +198,7 @@ def config_dict(args):
 def run_ours(args, rank, world, local_rank):
     import torch
     import vqcb200 as V
-    from vqcb200 import _lib
+    from vqcb200 import _lib, replicas
     from vqcb200 import workloads as W
     from vqcb200.circuit import Packed
 
@@ -231,8 +231,7 @@ def run_ours(args, rank, world, local_rank):
                 V.energy_and_gradient(H, circuit, psi0)
             else:
                 grad_call(psi0, grads, energy)
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         if profile:
             _lib.profile_enable(True)
@@ -253,10 +252,8 @@ def run_ours(args, rank, world, local_rank):
             _lib.profile_enable(False)
         ms = start.elapsed_time(end) / steps
         if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            torch.distributed.barrier()
-            ms = float(t.item())
+            ms = replicas.max_over_ranks(ms, device="cuda")  # slowest replica
+            replicas.barrier()
         return ms, prof, complex(energy[0], energy[1]), grads
 
     psi32 = make_state(np.complex64)
@@ -578,11 +575,10 @@ def main():
         run_serve(args, local_rank)
         return
     if world > 1:
-        import datetime
-
         import torch
+        from vqcb200 import replicas
         torch.cuda.set_device(local_rank)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        replicas.init_from_env("nccl")
     try:
         run_ours(args, rank, world, local_rank)
     finally:
