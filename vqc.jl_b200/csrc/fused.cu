@@ -283,7 +283,9 @@ struct MinBlocks {
   static constexpr int value = 2;
 };
 
-template <class R, int M, bool ADJ>
+// GEN = false: a pass made of one-qubit ops only (the common case of
+// parameterised circuits), compiled without the two-qubit and diagonal paths.
+template <class R, int M, bool ADJ, bool GEN = true>
 __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __restrict__ lam,
                                           const DevPass* __restrict__ pass, const DevStage* __restrict__ stages,
                                           const DevOp* __restrict__ ops, const cplx<R>* __restrict__ pool,
@@ -353,10 +355,11 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
         }
         const uint32_t cm = (uint32_t)hd.z, cv = (uint32_t)hd.w;
         const C* U = pool + hd.y;
-        if (type == kOpU1) {
+        if (!GEN || type == kOpU1) {
           const bool acc = ADJ && (code & kCodeAcc);
           dispatch_u1<ADJ, R>((code >> 4) & 3, code & kCodeCtl, (code >> 11) & 7, v, w, U, cm, cv, tthr, dep, acc,
                               (code >> 14) & 3, sacc, acc ? (op->slot) : 0, NW);
+        } else if (!GEN) {
         } else if (type == kOpU2) {
           dispatch_u2<ADJ, R>((code >> 4) & 3, (code >> 6) & 3, v, w, U, cm, cv, tthr, dep);
         } else {
@@ -438,11 +441,11 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
 }
 
 // One pass of one state (the single-request path).
-template <class R, int M, bool ADJ>
+template <class R, int M, bool ADJ, bool GEN>
 __global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
     k_tile(cplx<R>* psi, cplx<R>* lam, const DevPass* pass, const DevStage* stages, const DevOp* ops,
            const cplx<R>* pool, double* partials) {
-  tile_body<R, M, ADJ>(psi, lam, pass, stages, ops, pool, partials, gridDim.x);
+  tile_body<R, M, ADJ, GEN>(psi, lam, pass, stages, ops, pool, partials, gridDim.x);
 }
 
 template <class R, int M, bool ADJ>
@@ -799,7 +802,7 @@ template <class R, int M, bool ADJ>
 static int tile_grid(int device, const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t smem = pass_smem<R, M, ADJ>(ps);
-  auto kfun = k_tile<R, M, ADJ>;
+  auto kfun = ps.general ? k_tile<R, M, ADJ, true> : k_tile<R, M, ADJ, false>;
   cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, NT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
@@ -811,7 +814,7 @@ static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, con
                        const void* pool, double* partials, int grid, const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t smem = pass_smem<R, M, ADJ>(ps);
-  auto kfun = k_tile<R, M, ADJ>;
+  auto kfun = ps.general ? k_tile<R, M, ADJ, true> : k_tile<R, M, ADJ, false>;
   VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
   ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward",
                  (double)(ADJ ? 4 : 2) * h->size() * sizeof(cplx<R>));
@@ -961,6 +964,9 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
     locs[pi].shape.nstages = (int)ds.size();
     locs[pi].shape.nops = P.nops;
     locs[pi].shape.npool = P.npool;
+    locs[pi].shape.general = false;
+    for (const DevOp& o : dops)
+      if ((o.code & 15) != kOpU1) locs[pi].shape.general = true;
     locs[pi].row0 = row;
     row += slot;
     locs[pi].nslots = slot;

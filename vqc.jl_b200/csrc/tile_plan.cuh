@@ -91,6 +91,7 @@ struct FOp {
 
 struct PassShape {
   int nslots = 0, nstages = 0, nops = 0, npool = 0;
+  bool general = true;  // false: every op of the pass is a one-qubit op
 };
 
 // An accumulating op of the reverse sweep and the row of 8 doubles (the
