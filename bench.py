@@ -178,8 +178,10 @@ def run_reference(args, rank, world):
     value = float(np.median(vals))
     sample = ("per step: 2 rotations + 1 CRX forward and reverse sweep and one XXZ key at n=26, FP32 amplitudes "
               "(the reference's ComplexF32 path, FP32 accumulation), scaled to 20x(78 rotations + 25 CRX) + 25 keys")
+    # a step is the bounded sample; value is the sample's rate scaled to whole gradients
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(args.steps, 1),
+            "ms_per_gradient_extrapolated": 1000.0 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64",
             "data": "synthetic (seeded)", "config": config_dict(args),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
