@@ -28,10 +28,12 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <type_traits>
 
 #include "engine.h"
 #include "subspace.cuh"
 #include "tile_plan.cuh"
+#include "tile_f32.cuh"
 
 namespace vqc {
 
@@ -119,12 +121,6 @@ __device__ __forceinline__ void flush_acc(const R (&a)[8], double* sacc, int slo
 }
 
 // one-qubit op on register slot RR, both states in ADJ mode
-// One-qubit matrix forms (read off the matrix on the host): general complex;
-// "RI" = real diagonal and imaginary off-diagonal (RX-like); real (RY-like);
-// diagonal (RZ / phase); the exact swap [[0,1],[1,0]] (X, the CNOT/Toffoli target).
-enum { kFormGen = 0, kFormRI = 1, kFormReal = 2, kFormDiag = 3, kFormSwap = 4 };
-// Reduced-matrix entries a parameter's D touches: all four, off-diagonal, diagonal.
-enum { kAccFull = 0, kAccOff = 1, kAccDiag = 2 };
 
 template <int FORM, class C>
 __device__ __forceinline__ void u1_apply(C& x0, C& x1, C u00, C u01, C u10, C u11) {
@@ -276,11 +272,20 @@ __device__ __forceinline__ void dispatch_u2(int ra, int rb, cplx<R> (&v)[16], cp
 }
 
 // The tile kernel: one launch per pass, persistent over the tiles.
-// Resident CTAs per SM the register budget is sized for (three resident
-// forward CTAs measured slower than two).
+// Resident CTAs per SM the register budget is sized for.
+#ifndef VQC_MINB_F32_FWD
+#define VQC_MINB_F32_FWD 3
+#endif
+#ifndef VQC_MINB_F32_ADJ
+#define VQC_MINB_F32_ADJ 1
+#endif
 template <class R, bool ADJ>
 struct MinBlocks {
   static constexpr int value = 2;
+};
+template <bool ADJ>
+struct MinBlocks<float, ADJ> {
+  static constexpr int value = ADJ ? VQC_MINB_F32_ADJ : VQC_MINB_F32_FWD;
 };
 
 // GEN = false: a pass made of one-qubit ops only (the common case of
@@ -440,12 +445,22 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
   }
 }
 
-// One pass of one state (the single-request path).
+// One pass of one state (the single-request path).  FP32 states run the
+// packed body (tile_f32.cuh), FP64 states the body above.
+template <class R, int M, bool ADJ, bool GEN>
+__device__ __forceinline__ void tile_run(cplx<R>* psi, cplx<R>* lam, const DevPass* pass, const void* stages,
+                                         const DevOp* ops, const cplx<R>* pool, double* partials, int ncta) {
+  if constexpr (std::is_same<R, float>::value)
+    f32t::tile_body<M, ADJ, GEN>(psi, lam, pass, (const DevStageF*)stages, ops, pool, partials, ncta);
+  else
+    tile_body<R, M, ADJ, GEN>(psi, lam, pass, (const DevStage*)stages, ops, pool, partials, ncta);
+}
+
 template <class R, int M, bool ADJ, bool GEN>
 __global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
-    k_tile(cplx<R>* psi, cplx<R>* lam, const DevPass* pass, const DevStage* stages, const DevOp* ops,
+    k_tile(cplx<R>* psi, cplx<R>* lam, const DevPass* pass, const void* stages, const DevOp* ops,
            const cplx<R>* pool, double* partials) {
-  tile_body<R, M, ADJ, GEN>(psi, lam, pass, stages, ops, pool, partials, gridDim.x);
+  tile_run<R, M, ADJ, GEN>(psi, lam, pass, stages, ops, pool, partials, gridDim.x);
 }
 
 template <class R, int M, bool ADJ>
@@ -453,8 +468,8 @@ __global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
     k_tile_batch(const TileItem* __restrict__ items) {
   const TileItem it = items[blockIdx.y];
   if ((int)blockIdx.x >= it.ncta) return;
-  tile_body<R, M, ADJ>((cplx<R>*)it.psi, (cplx<R>*)it.lam, it.pass, it.stages, it.ops, (const cplx<R>*)it.pool,
-                       it.partials, it.ncta);
+  tile_run<R, M, ADJ, true>((cplx<R>*)it.psi, (cplx<R>*)it.lam, it.pass, it.stages, it.ops, (const cplx<R>*)it.pool,
+                            it.partials, it.ncta);
 }
 
 // Sums the per-CTA partials over the grid in a fixed order: block = slot.
@@ -704,24 +719,41 @@ static void plan_passes(int n, const TileConfig& tc, bool adj, std::vector<PItem
 }
 
 // Conflict check of a register-bit set for the shared-memory swizzle.
+// FP64: 16-byte amplitudes, quarter-warps over the tile swizzle Swz<double>.
+// FP32 (packed): 16-byte pairs, the lowest three thread bits (tile bits
+// outside rs, ascending) must fall in distinct classes of the pair swizzle,
+// class = (tile bit - 1) mod 3.
 static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype) {
+  if (dtype == VQC_C64) {
+    int seen = 0, k = 0;
+    for (int b = 1; b < M && k < 3; ++b) {
+      if (std::find(rs.begin(), rs.end(), b) != rs.end()) continue;
+      const int res = (b - 1) % 3;
+      if (seen >> res & 1) return false;
+      seen |= 1 << res;
+      ++k;
+    }
+    return true;
+  }
   std::vector<int> lanes;
-  for (int b = 0; b < M && (int)lanes.size() < (dtype == VQC_C64 ? 4 : 3); ++b)
+  for (int b = 0; b < M && (int)lanes.size() < 3; ++b)
     if (std::find(rs.begin(), rs.end(), b) == rs.end()) lanes.push_back(b);
   int seen = 0;
   for (int b : lanes) {
-    int res;
-    if (dtype == VQC_C64)
-      res = b < 4 ? b : (b < 8 ? b - 4 : -1);
-    else
-      res = b < 3 ? b : (b < 9 ? (b - 3) % 3 : -1);
+    const int res = b < 3 ? b : (b < 9 ? (b - 3) % 3 : -1);
     if (res < 0 || (seen >> res & 1)) return false;
     seen |= 1 << res;
   }
   return true;
 }
 
+// Cuts a pass into stages: runs of ops whose target bits fit the register
+// set (4 tile bits; for FP32 tile bit 0 is always one of them, the lane bit
+// of the packed layout).  The free bits left over are filled preferring the
+// stage's control bits (register controls are compile-time cases in the FP32
+// body), then a bank-conflict-free layout.
 static void plan_stages(PlanPass& p, int M, int dtype) {
+  const bool lane0 = dtype == VQC_C64;
   std::map<int, int> tbit;  // global qubit -> tile bit
   for (int b = 0; b < (int)p.tile_q.size(); ++b) tbit[p.tile_q[b]] = b;
   std::vector<int> pending(p.ops.size());
@@ -731,6 +763,7 @@ static void plan_stages(PlanPass& p, int M, int dtype) {
     uint64_t blocked = 0;
     std::vector<int> rest;
     std::vector<int> rs;
+    if (lane0) rs.push_back(0);
     for (int oi : pending) {
       const FOp& f = p.ops[oi];
       if (f.qubits & blocked) {
@@ -752,10 +785,20 @@ static void plan_stages(PlanPass& p, int M, int dtype) {
         rest.push_back(oi);
       }
     }
-    // fill the register set to 4 bits, preferring a conflict-free layout
+    // fill the register set to 4 bits: control bits of the stage's ops first
     std::vector<int> cand;
+    for (int oi : st.ops) {
+      const FOp& f = p.ops[oi];
+      for (int q = 0; q < 64; ++q)
+        if ((f.cmask >> q & 1) && tbit.count(q)) {
+          const int b = tbit[q];
+          if (std::find(rs.begin(), rs.end(), b) == rs.end() && std::find(cand.begin(), cand.end(), b) == cand.end())
+            cand.push_back(b);
+        }
+    }
     for (int b = 0; b < M; ++b)
-      if (std::find(rs.begin(), rs.end(), b) == rs.end()) cand.push_back(b);
+      if (std::find(rs.begin(), rs.end(), b) == rs.end() && std::find(cand.begin(), cand.end(), b) == cand.end())
+        cand.push_back(b);
     const int need_more = kRegBits - (int)rs.size();
     std::vector<int> best;
     bool found = false;
@@ -795,7 +838,7 @@ static size_t pass_smem(const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t npool = (size_t)ps.npool * sizeof(cplx<R>);
   return tile_bytes<R, M, ADJ>() + (ADJ ? (size_t)ps.nslots * (NT / 32) * 8 * sizeof(double) : 0) +
-         sizeof(DevStage) * ps.nstages + sizeof(DevOp) * ps.nops + ((npool + 15) & ~size_t(15));
+         (std::is_same<R, float>::value ? sizeof(DevStageF) : sizeof(DevStage)) * ps.nstages + sizeof(DevOp) * ps.nops + ((npool + 15) & ~size_t(15));
 }
 
 template <class R, int M, bool ADJ>
@@ -810,7 +853,7 @@ static int tile_grid(int device, const PassShape& ps) {
 }
 
 template <class R, int M, bool ADJ>
-static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, const DevStage* ds, const DevOp* dops,
+static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, const void* ds, const DevOp* dops,
                        const void* pool, double* partials, int grid, const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t smem = pass_smem<R, M, ADJ>(ps);
@@ -849,6 +892,158 @@ static int acc_kind(const FOp& f) {
   return kAccFull;
 }
 
+// One stage of the FP32 (packed) tile body: its DevStageF tables, its ops
+// (j-bit targets, register controls as compile-time cases or a mask, the
+// coefficient layouts of tile_f32.cuh) and their pool blocks.
+static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint64_t tile_mask,
+                      std::map<int, int>& tbit, bool adj, int& slot, int row, std::vector<DevStageF>& ds,
+                      std::vector<DevOp>& dops, std::vector<float2>& pool, size_t pool_begin,
+                      std::vector<AccRef>* accs) {
+  DevStageF s{};
+  const std::vector<int>& rs = st.rs;  // ascending, rs[0] = tile bit 0
+  uint32_t rsmask = 0;
+  for (int b : rs) rsmask |= 1u << b;
+  uint32_t dep[16];
+  for (int j = 0; j < 16; ++j) {
+    uint32_t t = 0;
+    for (int i = 0; i < kRegBits; ++i)
+      if (j >> i & 1) t |= 1u << rs[i];
+    dep[j] = t;
+    s.dep[j] = t;
+  }
+  std::vector<int> thr;
+  for (int b = 0; b < M; ++b)
+    if (!(rsmask >> b & 1)) thr.push_back(b);
+  auto gq = [&](uint32_t t) {
+    int64_t g = 0;
+    for (int b = 0; b < M; ++b)
+      if (t >> b & 1) g |= int64_t(1) << p.tile_q[b];
+    return g;
+  };
+  for (int k = 0; k < 2; ++k)
+    for (int nib = 0; nib < 16; ++nib) {
+      uint32_t t = 0;
+      for (int i = 0; i < 4; ++i)
+        if ((nib >> i & 1) && 4 * k + i < (int)thr.size()) t |= 1u << thr[4 * k + i];
+      s.thr[k][nib] = t;
+      s.swt[k][nib] = f32t::swz_pair(t >> 1);
+      s.gthr[k][nib] = gq(t);
+    }
+  for (int m = 0; m < 8; ++m) {
+    s.swm[m] = f32t::swz_pair(dep[2 * m] >> 1);
+    s.gdep[m] = gq(dep[2 * m]);
+  }
+  auto jbit = [&](int b) { return (int)(std::find(rs.begin(), rs.end(), b) - rs.begin()); };
+  auto put = [&](double a, double b) { pool.push_back(make_float2((float)a, (float)b)); };
+  auto dup = [&](double a) { put(a, a); };
+  s.op_begin = (int)dops.size();
+  for (int oi : st.ops) {
+    const FOp& f = p.ops[oi];
+    DevOp o{};
+    o.code = f.kind;
+    o.slot = -1;
+    std::vector<std::pair<int, int>> rc;  // register controls: (j-bit, value)
+    for (int q = 0; q < n; ++q) {
+      if (!(f.cmask >> q & 1)) continue;
+      const int v = (int)(f.cval >> q & 1);
+      if (tile_mask >> q & 1) {
+        const int b = tbit[q];
+        if (rsmask >> b & 1) {
+          rc.push_back({jbit(b), v});
+        } else {
+          o.cmask |= 1u << b;
+          if (v) o.cval |= 1u << b;
+        }
+      } else {
+        o.gmask |= 1ull << q;
+        if (v) o.gval |= 1ull << q;
+      }
+    }
+    uint32_t rmask = 0;
+    for (int j = 0; j < 16; ++j) {
+      bool ok = true;
+      for (auto& c : rc) ok = ok && ((j >> c.first & 1) == c.second);
+      if (ok) rmask |= 1u << j;
+    }
+    o.rmask = (int32_t)rmask;
+    int rctl = 0;
+    if (!rc.empty()) rctl = (rc.size() == 1 && rc[0].second == 1) ? rc[0].first + 1 : 7;
+    if (o.cmask) o.code |= kCodeCtl;
+    if (o.gmask) o.code |= kCodeGCtl;
+    while (pool.size() % 2) put(0, 0);  // each op's block starts on 16 bytes
+    o.mat = (int)(pool.size() - pool_begin);
+    if (f.kind == kOpU1) {
+      const int tb = jbit(tbit[f.tq[0]]), form = u1_form(f.mat);
+      o.code |= (tb << 4) | (form << 11) | (rctl << 16);
+      if (adj && f.acc) o.code |= acc_kind(f) << 14;
+      const cd u00 = f.mat[0], u01 = f.mat[1], u10 = f.mat[2], u11 = f.mat[3];
+      if (tb != 0) {
+        switch (form) {
+          case kFormGen:
+            for (const cd& u : {u00, u01, u10, u11}) {
+              dup(u.real());
+              dup(u.imag());
+              dup(-u.imag());
+            }
+            break;
+          case kFormRI:
+            dup(u00.real()), dup(u01.imag()), dup(-u01.imag()), dup(u11.real()), dup(u10.imag()), dup(-u10.imag());
+            break;
+          case kFormReal: dup(u00.real()), dup(u01.real()), dup(u10.real()), dup(u11.real()); break;
+          case kFormDiag:
+            dup(u00.real()), dup(u00.imag()), dup(-u00.imag()), dup(u11.real()), dup(u11.imag()), dup(-u11.imag());
+            break;
+          default: break;
+        }
+      } else {
+        switch (form) {
+          case kFormGen:
+            put(u00.real(), u11.real()), put(u01.real(), u10.real()), put(u00.imag(), u11.imag());
+            put(-u00.imag(), -u11.imag()), put(u01.imag(), u10.imag()), put(-u01.imag(), -u10.imag());
+            break;
+          case kFormRI: put(u00.real(), u11.real()), put(-u01.imag(), -u10.imag()), put(u01.imag(), u10.imag()); break;
+          case kFormReal: put(u00.real(), u11.real()), put(u01.real(), u10.real()); break;
+          case kFormDiag:
+            put(u00.real(), u11.real()), put(u00.imag(), u11.imag()), put(-u00.imag(), -u11.imag());
+            break;
+          default: break;
+        }
+      }
+    } else {
+      if (f.kind == kOpU2) o.code |= (jbit(tbit[f.tq[0]]) << 4) | (jbit(tbit[f.tq[1]]) << 6);
+      for (const cd& c : f.mat) put(c.real(), c.imag());
+    }
+    o.nd = f.nd;
+    for (int i = 0; i < 5; ++i) {
+      o.dbit[i] = -1;
+      o.dglob[i] = 0;
+      if (i < f.nd) {
+        if (tile_mask >> f.dq[i] & 1)
+          o.dbit[i] = tbit[f.dq[i]];
+        else
+          o.dglob[i] = f.dq[i];
+      }
+    }
+    if (adj && f.acc) {
+      o.slot = slot++;
+      if (f.kind == kOpDiag) {
+        // the accumulation runs as its own op right after the diagonal
+        dops.push_back(o);
+        DevOp a = o;
+        a.code = (a.code & ~15) | kOpAccD;
+        dops.push_back(a);
+        if (accs) accs->push_back(AccRef{row + o.slot, f});
+        continue;
+      }
+      if (accs) accs->push_back(AccRef{row + o.slot, f});
+      o.code |= kCodeAcc;
+    }
+    dops.push_back(o);
+  }
+  s.op_end = (int)dops.size();
+  ds.push_back(s);
+}
+
 template <class R, int M, bool ADJ>
 static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, SerialPlan& sp, std::vector<AccRef>* accs) {
   Device d;
@@ -873,7 +1068,12 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
     int slot = 0;
     while ((pool.size() * sizeof(cplx<R>)) % 16) pool.push_back(mkc<R>(R(0), R(0)));
     const size_t pool_begin = pool.size();
+    std::vector<DevStageF> dsf;
     for (const PlanStage& st : p.stages) {
+      if constexpr (std::is_same<R, float>::value) {
+        stage_f32(p, st, M, n, tile_mask, tbit, ADJ, slot, row, dsf, dops, pool, pool_begin, accs);
+        continue;
+      }
       DevStage s{};
       uint32_t rsmask = 0;
       for (int b : st.rs) rsmask |= 1u << b;
@@ -961,7 +1161,7 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
     P.npool = (int)(pool.size() - pool_begin);
     locs[pi].pool_begin = pool_begin;
     locs[pi].shape.nslots = ADJ ? slot : 0;
-    locs[pi].shape.nstages = (int)ds.size();
+    locs[pi].shape.nstages = (int)p.stages.size();
     locs[pi].shape.nops = P.nops;
     locs[pi].shape.npool = P.npool;
     locs[pi].shape.general = false;
@@ -972,30 +1172,16 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
     locs[pi].nslots = slot;
     // stage indices are local to this pass's stage array
     P.stage_begin = 0;
-    P.stage_end = (int)ds.size();
+    P.stage_end = (int)p.stages.size();
     locs[pi].pass = d.put(&P, 1);
-    locs[pi].stages = d.put(ds.data(), ds.size());
+    if constexpr (std::is_same<R, float>::value)
+      locs[pi].stages = d.put(dsf.data(), dsf.size());
+    else
+      locs[pi].stages = d.put(ds.data(), ds.size());
     // op indices in stages are local to this pass's op array
     locs[pi].ops = d.put(dops.data(), std::max<size_t>(dops.size(), 1));
   }
-  {
-    long long np = 0, ns = 0, no = 0, nsa = 0;
-    for (auto& p : passes) {
-      if (p.standalone) {
-        ++nsa;
-        continue;
-      }
-      ++np;
-      ns += (long long)p.stages.size();
-      no += (long long)p.ops.size();
-    }
-    prof_note(ADJ ? "plan_adjoint_passes" : "plan_forward_passes", np);
-    prof_note(ADJ ? "plan_adjoint_stages" : "plan_forward_stages", ns);
-    prof_note(ADJ ? "plan_adjoint_ops" : "plan_forward_ops", no);
-    prof_note("plan_standalone_gates", nsa);
-  }
-  for (int i = 0; i < 2; ++i) pool.push_back(mkc<R>(R(0), R(0)));  // the staging copy reads whole 16-byte words
-  for (int i = 0; i < 2; ++i) pool.push_back(mkc<R>(R(0), R(0)));  // the staging copy reads whole 16-byte words
+  for (int i = 0; i < 4; ++i) pool.push_back(mkc<R>(R(0), R(0)));  // the staging copy reads whole 16-byte words
   sp.pool_off = d.put(pool.data(), pool.size());
   sp.rows = row;
   sp.buf.swap(d.buf);
@@ -1018,6 +1204,38 @@ static void note_plan(bool adj, const std::vector<PlanPass>& passes) {
   prof_note("plan_standalone_gates", nsa);
 }
 
+template <int M, bool ADJ>
+static int jit_grid(int device, const void* k, const PassShape& ps) {
+  constexpr int NT = 1 << (M - kRegBits);
+  const size_t smem = pass_smem<float, M, ADJ>(ps);
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return device_info(device).sms * per_sm;
+}
+
+template <int M, bool ADJ>
+static int launch_tile_jit(vqc_state h, const void* k, void* psi, void* lam, const DevPass* dp, const void* ds,
+                           const DevOp* dops, const void* pool, double* partials, int grid, const PassShape& ps) {
+  constexpr int NT = 1 << (M - kRegBits);
+  const size_t smem = pass_smem<float, M, ADJ>(ps);
+  VQC_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
+  ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward", (double)(ADJ ? 4 : 2) * h->size() * sizeof(float2));
+  void* args[] = {&psi, &lam, (void*)&dp, (void*)&ds, (void*)&dops, (void*)&pool, &partials};
+  VQC_CK(cudaLaunchKernel(k, dim3(grid), dim3(NT), args, smem, h->stream));
+  return VQC_OK;
+}
+
+// JIT tile passes for FP32 states of at least 2^18 amplitudes (VQC_JIT=auto),
+// all FP32 tile passes (on), none (off).
+static bool use_jit(const vqc_state h) {
+  const int mode = jit_mode();
+  return h->dtype == VQC_C64 && (mode == 1 || (mode == 2 && h->nq >= 18)) && jit_available();
+}
+
 template <class R, int M, bool ADJ>
 static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
                     std::vector<AccRef>* accs, double* rows_dev) {
@@ -1027,6 +1245,27 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   note_plan(ADJ, passes);
   const std::vector<PassLoc>& locs = sp.locs;
   const size_t pool_off = sp.pool_off;
+  // run-time specialised kernels (FP32), one per pass structure
+  std::vector<const void*> jk(passes.size(), nullptr);
+  if constexpr (std::is_same<R, float>::value) {
+    if (use_jit(h)) {
+      std::vector<std::string> srcs(passes.size());
+      for (size_t pi = 0; pi < passes.size(); ++pi)
+        if (!locs[pi].standalone)
+          srcs[pi] = jit_pass_source(M, ADJ, (const DevStageF*)(sp.buf.data() + locs[pi].stages),
+                                     locs[pi].shape.nstages, (const DevOp*)(sp.buf.data() + locs[pi].ops));
+      jit_kernels(srcs, jk);
+    }
+  }
+  std::vector<int> grids(passes.size(), 0);
+  for (size_t pi = 0; pi < passes.size(); ++pi) {
+    if (locs[pi].standalone) continue;
+    int g = 0;
+    if constexpr (std::is_same<R, float>::value)
+      if (jk[pi]) g = jit_grid<M, ADJ>(h->device, jk[pi], locs[pi].shape);
+    if (!g) g = tile_grid<R, M, ADJ>(h->device, locs[pi].shape);
+    grids[pi] = (int)std::min<int64_t>(g, locs[pi].ntiles);
+  }
   int rc = upload_ops(h, sp.buf.data(), sp.buf.size());
   if (rc) return rc;
   const unsigned char* base = (const unsigned char*)h->opbuf;
@@ -1034,8 +1273,7 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   size_t need = 0;
   for (size_t pi = 0; pi < passes.size(); ++pi)
     if (!locs[pi].standalone && locs[pi].nslots > 0)
-      need = std::max(need, (size_t)tile_grid<R, M, ADJ>(h->device, locs[pi].shape) * locs[pi].nslots * 8 *
-                                sizeof(double));
+      need = std::max(need, (size_t)grids[pi] * locs[pi].nslots * 8 * sizeof(double));
   double* partials = nullptr;
   if (ADJ && need > 0) {
     if (need > h->fused_scratch_bytes) {
@@ -1060,12 +1298,18 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
       continue;
     }
     const int nslots = locs[pi].nslots;
-    const int grid = (int)std::min<int64_t>(tile_grid<R, M, ADJ>(h->device, locs[pi].shape), locs[pi].ntiles);
-    if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, (const DevPass*)(base + locs[pi].pass),
-                                      (const DevStage*)(base + locs[pi].stages), (const DevOp*)(base + locs[pi].ops),
-                                      base + pool_off + locs[pi].pool_begin * sizeof(cplx<R>), partials, grid,
-                                      locs[pi].shape)))
+    const int grid = grids[pi];
+    const DevPass* dp = (const DevPass*)(base + locs[pi].pass);
+    const void* ds = (const void*)(base + locs[pi].stages);
+    const DevOp* dops = (const DevOp*)(base + locs[pi].ops);
+    const void* dpool = base + pool_off + locs[pi].pool_begin * sizeof(cplx<R>);
+    if (jk[pi]) {
+      if constexpr (std::is_same<R, float>::value)
+        if ((rc = launch_tile_jit<M, ADJ>(h, jk[pi], psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape)))
+          return rc;
+    } else if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape))) {
       return rc;
+    }
     if (ADJ && nslots > 0) {
       k_reduce_slots<<<nslots, 256, 0, h->stream>>>(partials, grid, nslots, locs[pi].row0, rows_dev);
       VQC_CK(cudaGetLastError());

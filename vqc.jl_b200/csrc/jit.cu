@@ -1,0 +1,268 @@
+// Run-time specialised FP32 tile kernels.
+//
+// The interpreted tile kernel (tile_f32.cuh, interp_ops) decodes every op of
+// a pass at run time; on sm_100 that costs about as many integer and move
+// instructions as the op's packed FMAs, because each of the many op variants
+// leaves the amplitudes in different registers.  A pass's *structure* (its
+// stages, and per op the type, target and control bits, matrix form and
+// accumulated entries) is known when the circuit is planned, and the same
+// structures recur from layer to layer and from call to call.  So the pass
+// is written out as straight-line CUDA (every op a compile-time variant of
+// the same device functions), compiled with NVRTC for sm_100a once per
+// structure, and cached for the life of the process.  Everything that varies
+// between calls with the same structure (angles, masks, addresses, slots)
+// stays run-time data in the pass's descriptors, exactly as the interpreter
+// reads them.
+//
+// VQC_JIT=0 / off: never (the interpreter runs every pass); 1 / on: every
+// FP32 tile pass; auto (default): passes of states with at least 2^18
+// amplitudes.  If NVRTC cannot be loaded, or a compilation fails, the pass
+// runs on the interpreter (also a GPU kernel).
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <thread>
+
+#include "tile_plan.cuh"
+
+namespace vqc {
+
+namespace {
+
+#include "jit_src.inc"  // kJitTileDev, kJitTileF32: the device headers as text (generated at build time)
+
+struct Nvrtc {
+  bool ok = false;
+  decltype(&nvrtcCreateProgram) create = nullptr;
+  decltype(&nvrtcCompileProgram) compile = nullptr;
+  decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
+  decltype(&nvrtcGetCUBIN) cubin = nullptr;
+  decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
+  decltype(&nvrtcGetProgramLog) log = nullptr;
+  decltype(&nvrtcDestroyProgram) destroy = nullptr;
+};
+
+const Nvrtc& nvrtc() {
+  static Nvrtc n = [] {
+    Nvrtc r;
+    std::vector<std::string> cands = {"libnvrtc.so.12", "libnvrtc.so"};
+    for (const char* env : {"CUDA_HOME", "CUDA_PATH"})
+      if (const char* h = std::getenv(env)) cands.push_back(std::string(h) + "/lib64/libnvrtc.so.12");
+    cands.push_back("/usr/local/cuda/lib64/libnvrtc.so.12");
+    void* h = nullptr;
+    for (const std::string& c : cands)
+      if ((h = dlopen(c.c_str(), RTLD_NOW | RTLD_LOCAL))) break;
+    if (!h) return r;
+    r.create = (decltype(r.create))dlsym(h, "nvrtcCreateProgram");
+    r.compile = (decltype(r.compile))dlsym(h, "nvrtcCompileProgram");
+    r.cubin_size = (decltype(r.cubin_size))dlsym(h, "nvrtcGetCUBINSize");
+    r.cubin = (decltype(r.cubin))dlsym(h, "nvrtcGetCUBIN");
+    r.log_size = (decltype(r.log_size))dlsym(h, "nvrtcGetProgramLogSize");
+    r.log = (decltype(r.log))dlsym(h, "nvrtcGetProgramLog");
+    r.destroy = (decltype(r.destroy))dlsym(h, "nvrtcDestroyProgram");
+    r.ok = r.create && r.compile && r.cubin_size && r.cubin && r.log_size && r.log && r.destroy;
+    return r;
+  }();
+  return n;
+}
+
+struct Entry {
+  cudaLibrary_t lib = nullptr;
+  cudaKernel_t kernel = nullptr;
+  bool failed = false;
+  std::string log;
+};
+
+std::mutex g_mu;
+std::map<std::string, Entry>& cache() {
+  static std::map<std::string, Entry> c;
+  return c;
+}
+
+int env_int(const char* name, int dflt) {
+  const char* v = std::getenv(name);
+  return v && *v ? std::atoi(v) : dflt;
+}
+
+// NVRTC -> cubin for one source (thread-safe; no CUDA calls).
+bool compile_one(const std::string& src, std::vector<char>& cubin, std::string& log) {
+  const Nvrtc& nv = nvrtc();
+  nvrtcProgram prog;
+  const char* hdrs[2] = {kJitTileDev, kJitTileF32};
+  const char* names[2] = {"tile_dev.cuh", "tile_f32.cuh"};
+  if (nv.create(&prog, src.c_str(), "vqc_pass.cu", 2, hdrs, names) != NVRTC_SUCCESS) {
+    log = "nvrtcCreateProgram failed";
+    return false;
+  }
+  std::vector<const char*> opts = {"-arch=sm_100a", "-std=c++17", "-lineinfo", "--extra-device-vectorization"};
+  if (env_int("VQC_JIT_VERBOSE", 0)) opts.push_back("--ptxas-options=-v");
+  const nvrtcResult rc = nv.compile(prog, (int)opts.size(), opts.data());
+  size_t ls = 0;
+  nv.log_size(prog, &ls);
+  log.assign(ls, '\0');
+  if (ls) nv.log(prog, &log[0]);
+  bool ok = rc == NVRTC_SUCCESS;
+  if (ok) {
+    size_t cs = 0;
+    ok = nv.cubin_size(prog, &cs) == NVRTC_SUCCESS && cs > 0;
+    if (ok) {
+      cubin.resize(cs);
+      ok = nv.cubin(prog, cubin.data()) == NVRTC_SUCCESS;
+    }
+  }
+  nv.destroy(&prog);
+  return ok;
+}
+
+// The code of one op of a stage (o = its index in the pass's op array).
+void emit_op(std::ostringstream& os, const DevOp& op, int o) {
+  const int code = op.code, type = code & 15;
+  const bool ctl = code & kCodeCtl, gctl = code & kCodeGCtl, acc = code & kCodeAcc;
+  os << "    { const DevOp* op = x.ops + " << o << ";\n";
+  if (gctl) os << "      if ((x.base & op->gmask) == op->gval) {\n";
+  if (type == kOpU1) {
+    const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = (code >> 14) & 3;
+    const int cb = rctl == 0 ? -1 : rctl - 1;
+    os << "      const u64* c = reinterpret_cast<const u64*>(x.pool + op->mat);\n";
+    if (ctl) os << "      const bool run = (tthr & op->cmask) == op->cval;\n";
+    if (acc) os << "      float s8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};\n";
+    os << "      " << (ctl ? "if (run) " : "") << "{\n";
+    if (rctl == 7)
+      os << "        u1_masked<" << tb << ", " << form << ", ADJ>(v, w, c, (uint32_t)op->rmask);\n";
+    else
+      os << "        u1_static<" << tb << ", " << cb << ", " << form << ", ADJ>(v, w, c);\n";
+    if (acc) {
+      if (rctl == 7)
+        os << "        acc_masked<" << tb << ", " << kind << ">(v, w, (uint32_t)op->rmask, s8);\n";
+      else
+        os << "        acc_static<" << tb << ", " << cb << ", " << kind << ">(v, w, s8);\n";
+    }
+    os << "      }\n";
+    if (acc) os << "      flush8(s8, x.sacc, op->slot, NW);\n";
+  } else if (type == kOpU2) {
+    const int ja = (code >> 4) & 3, jb = (code >> 6) & 3;
+    if (ctl) os << "      if ((tthr & op->cmask) == op->cval)\n";
+    os << "      u2_op<" << ja << ", " << jb << ", ADJ>(v, w, x.pool + op->mat, (uint32_t)op->rmask);\n";
+  } else if (type == kOpDiag) {
+    os << "      diag_op<ADJ>(v, w, op, x.pool + op->mat, tthr, S->dep, x.base);\n";
+  } else {
+    os << "      float s8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};\n"
+       << "      accd_op(v, w, op, tthr, S->dep, x.base, s8);\n"
+       << "      flush8(s8, x.sacc, op->slot, NW);\n";
+  }
+  if (gctl) os << "      }\n";
+  os << "    }\n";
+}
+
+}  // namespace
+
+int jit_mode() {
+  const char* v = std::getenv("VQC_JIT");
+  if (!v || !*v || !std::strcmp(v, "auto")) return 2;
+  if (!std::strcmp(v, "0") || !std::strcmp(v, "off")) return 0;
+  return 1;
+}
+
+bool jit_available() { return nvrtc().ok; }
+
+int jit_min_blocks(bool adj) { return adj ? env_int("VQC_JIT_MINB_ADJ", 2) : env_int("VQC_JIT_MINB_FWD", 3); }
+
+std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops) {
+  std::ostringstream os;
+  const int NT = 1 << (M - kRegBits);
+  os << "#include \"tile_f32.cuh\"\n"
+     << "using namespace vqc;\nusing namespace vqc::f32t;\n"
+     << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj) << ")\n"
+     << "vqc_pass(float2* psi, float2* lam, const DevPass* pass, const DevStageF* stages, const DevOp* ops,\n"
+     << "         const float2* pool, double* partials) {\n"
+     << "  constexpr int M = " << M << ";\n  constexpr bool ADJ = " << (adj ? "true" : "false") << ";\n"
+     << "  constexpr int NW = TileCtx<M, ADJ>::NW;\n"
+     << "  __shared__ DevPass P;\n  __shared__ uint64_t s_inc, s_base0;\n"
+     << "  TileCtx<M, ADJ> x;\n"
+     << "  tile_setup<M, ADJ>(x, psi, lam, pass, stages, ops, pool, gridDim.x, P, s_inc, s_base0);\n"
+     << "  Pk v[8], w[8];\n"
+     << "  for (int it = 0; it < x.ntiles_here; ++it) {\n";
+  for (int s = 0; s < nst; ++s) {
+    os << "  {\n    const DevStageF* S = x.stages + " << s << ";\n"
+       << "    stage_load<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w);\n"
+       << "    const uint32_t tthr = S->thr[0][x.tlo] | S->thr[1][x.thi];\n    (void)tthr;\n";
+    for (int o = st[s].op_begin; o < st[s].op_end; ++o) emit_op(os, ops[o], o);
+    os << "    stage_store<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w);\n  }\n";
+  }
+  os << "    tile_next<M, ADJ>(x, s_inc);\n  }\n  tile_finish<M, ADJ>(x, partials);\n  (void)NW;\n}\n";
+  return os.str();
+}
+
+// Kernels for `srcs` (nullptr where unavailable): cached ones at once, the
+// rest compiled in parallel, then loaded.
+int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out) {
+  out.assign(srcs.size(), nullptr);
+  if (!jit_available()) return VQC_OK;
+  std::vector<size_t> todo;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::map<std::string, size_t> seen;
+    for (size_t i = 0; i < srcs.size(); ++i) {
+      if (srcs[i].empty()) continue;
+      auto it = cache().find(srcs[i]);
+      if (it != cache().end()) {
+        if (!it->second.failed) out[i] = (const void*)it->second.kernel;
+      } else if (!seen.count(srcs[i])) {
+        seen[srcs[i]] = i;
+        todo.push_back(i);
+      }
+    }
+  }
+  if (!todo.empty()) {
+    std::vector<std::vector<char>> bins(todo.size());
+    std::vector<std::string> logs(todo.size());
+    std::vector<char> ok(todo.size(), 0);
+    const int nthr = std::max(1, std::min<int>((int)todo.size(), (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    std::mutex qm;
+    size_t next = 0;
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&] {
+        while (true) {
+          size_t k;
+          {
+            std::lock_guard<std::mutex> lk(qm);
+            if (next >= todo.size()) return;
+            k = next++;
+          }
+          ok[k] = compile_one(srcs[todo[k]], bins[k], logs[k]);
+        }
+      });
+    for (auto& th : pool) th.join();
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (size_t k = 0; k < todo.size(); ++k) {
+      Entry e;
+      e.log = logs[k];
+      if (ok[k] && cudaLibraryLoadData(&e.lib, bins[k].data(), nullptr, nullptr, 0, nullptr, nullptr, 0) ==
+                       cudaSuccess &&
+          cudaLibraryGetKernel(&e.kernel, e.lib, "vqc_pass") == cudaSuccess) {
+        e.failed = false;
+      } else {
+        e.failed = true;
+        cudaGetLastError();
+        if (env_int("VQC_JIT_VERBOSE", 0)) fprintf(stderr, "vqc jit: compile failed:\n%s\n", e.log.c_str());
+      }
+      if (env_int("VQC_JIT_VERBOSE", 0) && !e.failed) fprintf(stderr, "vqc jit: %s\n", e.log.c_str());
+      cache()[srcs[todo[k]]] = e;
+    }
+    for (size_t i = 0; i < srcs.size(); ++i) {
+      if (srcs[i].empty()) continue;
+      auto it = cache().find(srcs[i]);
+      if (it != cache().end() && !it->second.failed) out[i] = (const void*)it->second.kernel;
+    }
+    prof_note("jit_compiled_passes", (long long)todo.size());
+  }
+  return VQC_OK;
+}
+
+}  // namespace vqc

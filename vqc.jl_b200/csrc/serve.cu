@@ -292,7 +292,7 @@ static void worker_main(vqc_server_s* s) {
       if (r->step < F) {
         const PassLoc& l = r->plan.fwd.locs[r->step];
         fwd_items[r->plan.M].push_back(TileItem{r->psi, nullptr, (const DevPass*)(img + l.pass),
-                                                (const DevStage*)(img + l.stages), (const DevOp*)(img + l.ops),
+                                                (const void*)(img + l.stages), (const DevOp*)(img + l.ops),
                                                 img + r->plan.fwd.pool_off + l.pool_begin * amp, nullptr, l.ntiles,
                                                 r->fwd_cap, 0});
         fwd_req[r->plan.M].push_back(r);
@@ -305,7 +305,7 @@ static void worker_main(vqc_server_s* s) {
         const PassLoc& l = r->plan.adj.locs[r->step - F - 1];
         const unsigned char* ai = img + r->off_adj;
         adj_items[r->plan.M].push_back(TileItem{r->psi, r->lam, (const DevPass*)(ai + l.pass),
-                                                (const DevStage*)(ai + l.stages), (const DevOp*)(ai + l.ops),
+                                                (const void*)(ai + l.stages), (const DevOp*)(ai + l.ops),
                                                 ai + r->plan.adj.pool_off + l.pool_begin * amp, r->partials,
                                                 l.ntiles, r->adj_cap, 0});
         adj_req[r->plan.M].push_back(r);

@@ -1,0 +1,86 @@
+// Device-side descriptors of the tile engine: the pass, stage and op
+// records the tile kernels read.  Self-contained (no host headers) so that the
+// run-time compiled pass kernels can include it as well.
+#pragma once
+
+#ifdef __CUDACC_RTC__
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+typedef unsigned int uint32_t;
+typedef int int32_t;
+#else
+#include <cstdint>
+#endif
+
+namespace vqc {
+
+constexpr int kRegBits = 4;  // 16 amplitudes per thread
+constexpr int kMaxSlots = 64;
+constexpr int kMaxOpsPerPass = 192;  // bounds the pass's descriptors staged in shared memory
+enum { kOpU1 = 1, kOpU2 = 2, kOpDiag = 3, kOpAccD = 4 };
+
+struct DevPass {
+  uint64_t nontile_mask;  // global bits enumerated by the tile counter
+  int64_t ntiles;
+  int32_t stage_begin, stage_end;
+  int32_t nslots;
+  int32_t nops;           // ops of this pass (copied to shared memory with the stages)
+  int32_t npool;          // matrix pool entries of this pass
+  int32_t pad;
+};
+
+struct alignas(16) DevStage {
+  uint32_t dep[16];    // tile index of register slot j (OR with the thread part)
+  int64_t gdep[16];    // global offset of register slot j
+  uint64_t gthr_mask;  // global qubits of the thread's tile bits
+  uint32_t thr_mask;   // tile bits held by the thread index, ascending
+  int32_t op_begin, op_end, pad;
+};
+
+// A stage of the FP32 (packed) tile body: tile bit 0 is always a register
+// bit (the lane bit inside each float4 pair), plus three free register bits.
+// Per-thread quantities are split into two tables indexed by the thread
+// index's low and high nibble (thread bits are at most 8).
+struct alignas(16) DevStageF {
+  int64_t gdep[8];       // global amplitude offset of register pair m (lane 0)
+  int64_t gthr[2][16];   // global offset of the thread's tile bits: [0][tid & 15] + [1][tid >> 4]
+  uint32_t thr[2][16];   // tile index of the thread's bits: [0][tid & 15] | [1][tid >> 4]
+  uint32_t swt[2][16];   // swizzled pair index of the thread's bits: [0][..] ^ [1][..]
+  uint32_t swm[8];       // swizzled pair index of register pair m
+  uint32_t dep[16];      // tile index of register amplitude j = lane + 2m
+  int32_t op_begin, op_end, pad0, pad1;
+};
+
+// code: bits 0-3 op type, 4-5 r0, 6-7 r1, 8 tile-bit controls, 9 non-tile
+// controls, 10 accumulate.  The first 16 bytes are read as one vector load.
+// In the FP32 body, r0/r1 are j-bits (0 = lane bit, 1..3 = free register
+// bits), cmask/cval hold only the controls on thread bits, and the controls
+// on register bits are bits 16-18 (0: none, 1..4: one control on j-bit
+// value-1 at |1>, 7: the amplitudes enabled in rmask).
+struct alignas(16) DevOp {
+  int32_t code;
+  int32_t mat;     // pool offset (complex elements)
+  uint32_t cmask, cval;  // controls on tile bits
+  uint64_t gmask, gval;  // controls on non-tile qubits
+  int32_t slot;    // accumulation slot or -1
+  int32_t nd;      // diagonal ops: number of qubits
+  int32_t dbit[5];  // tile bit of diagonal qubit i, or -1
+  int32_t dglob[5]; // global qubit of diagonal qubit i when not a tile bit
+  int32_t rmask;    // FP32 body: register amplitudes (pair representatives) the controls enable
+};
+constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
+// bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries accumulated
+// One-qubit matrix forms (read off the matrix on the host): general complex;
+// "RI" = real diagonal and imaginary off-diagonal (RX-like); real (RY-like);
+// diagonal (RZ / phase); the exact swap [[0,1],[1,0]] (X, the CNOT/Toffoli target).
+enum { kFormGen = 0, kFormRI = 1, kFormReal = 2, kFormDiag = 3, kFormSwap = 4 };
+// Reduced-matrix entries a parameter's D touches: all four, off-diagonal, diagonal.
+enum { kAccFull = 0, kAccOff = 1, kAccDiag = 2 };
+
+// Shared-memory bytes of the FP32 tile(s) of one pass.
+template <int M, bool ADJ>
+__host__ __device__ constexpr unsigned long long tile_bytes_f32() {
+  return (ADJ ? 2ull : 1ull) * (1ull << M) * 8ull;
+}
+
+}  // namespace vqc

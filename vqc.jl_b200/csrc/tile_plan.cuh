@@ -6,23 +6,9 @@
 #include <vector>
 
 #include "engine.h"
+#include "tile_dev.cuh"
 
 namespace vqc {
-
-constexpr int kRegBits = 4;  // 16 amplitudes per thread
-constexpr int kMaxSlots = 64;
-constexpr int kMaxOpsPerPass = 192;  // bounds the pass's descriptors staged in shared memory
-enum { kOpU1 = 1, kOpU2 = 2, kOpDiag = 3, kOpAccD = 4 };
-
-struct DevPass {
-  uint64_t nontile_mask;  // global bits enumerated by the tile counter
-  int64_t ntiles;
-  int32_t stage_begin, stage_end;
-  int32_t nslots;
-  int32_t nops;           // ops of this pass (copied to shared memory with the stages)
-  int32_t npool;          // matrix pool entries of this pass
-  int32_t pad;
-};
 
 // Shared-memory bytes of one pass: tiles, accumulation slots, and the pass's
 // own stage / op / matrix descriptors (read by every thread for every op, so
@@ -32,29 +18,6 @@ __host__ __device__ constexpr size_t tile_bytes() {
   return (size_t)(ADJ ? 2 : 1) * (size_t(1) << M) * sizeof(cplx<R>);
 }
 
-struct alignas(16) DevStage {
-  uint32_t dep[16];    // tile index of register slot j (OR with the thread part)
-  int64_t gdep[16];    // global offset of register slot j
-  uint64_t gthr_mask;  // global qubits of the thread's tile bits
-  uint32_t thr_mask;   // tile bits held by the thread index, ascending
-  int32_t op_begin, op_end, pad;
-};
-
-// code: bits 0-3 op type, 4-5 r0, 6-7 r1, 8 tile-bit controls, 9 non-tile
-// controls, 10 accumulate.  The first 16 bytes are read as one vector load.
-struct alignas(16) DevOp {
-  int32_t code;
-  int32_t mat;     // pool offset (complex elements)
-  uint32_t cmask, cval;  // controls on tile bits
-  uint64_t gmask, gval;  // controls on non-tile qubits
-  int32_t slot;    // accumulation slot or -1
-  int32_t nd;      // diagonal ops: number of qubits
-  int32_t dbit[5];  // tile bit of diagonal qubit i, or -1
-  int32_t dglob[5]; // global qubit of diagonal qubit i when not a tile bit
-};
-constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
-// bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries accumulated
-
 // One pass each of many states in one launch (the serving path): request
 // blockIdx.y, its tiles strided over its own `ncta` CTAs (fixed per request,
 // so its sums are grouped the same way whatever it is batched with); CTAs
@@ -63,7 +26,7 @@ struct TileItem {
   void* psi;
   void* lam;
   const DevPass* pass;
-  const DevStage* stages;
+  const void* stages;  // DevStage (FP64) or DevStageF (FP32)
   const DevOp* ops;
   const void* pool;
   double* partials;  // [ncta][nslots][8]
@@ -172,6 +135,14 @@ struct ReqPlan {
   PassShape fwd_max, adj_max;
   int64_t ntiles = 0;
 };
+
+// Run-time specialised FP32 tile kernels (jit.cu).
+int jit_mode();        // 0 off, 1 on, 2 auto (VQC_JIT)
+bool jit_available();  // NVRTC could be loaded
+int jit_min_blocks(bool adj);
+std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops);
+// Kernels for the given pass sources (nullptr for an empty source or a failed compile).
+int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out);
 
 int serve_build_plan(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
                      const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp);

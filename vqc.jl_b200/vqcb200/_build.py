@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libvqcb200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
-                "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
+                "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC, "-I", BUILD]
 
 
 def sources():
@@ -44,9 +44,29 @@ def _compile(src, extra):
     return obj, r.stderr
 
 
+JIT_HEADERS = [("kJitTileDev", "tile_dev.cuh"), ("kJitTileF32", "tile_f32.cuh")]
+
+
+def write_jit_sources():
+    """_build/jit_src.inc: the device headers the run-time compiled pass
+    kernels include, as C++ raw string literals (rewritten only on change)."""
+    out = os.path.join(BUILD, "jit_src.inc")
+    parts = ["// generated by vqcb200/_build.py from csrc/ (do not edit)\n"]
+    for name, f in JIT_HEADERS:
+        text = open(os.path.join(CSRC, f)).read()
+        if ")VQCJIT" in text:
+            raise RuntimeError("%s contains the raw-string delimiter" % f)
+        parts.append('static const char* %s = R"VQCJIT(%s)VQCJIT";\n' % (name, text))
+    data = "".join(parts)
+    if not os.path.exists(out) or open(out).read() != data:
+        with open(out, "w") as fh:
+            fh.write(data)
+
+
 def build(verbose=False, extra=()):
     """Compile every csrc/*.cu for sm_100a and link libvqcb200.so (incremental)."""
     os.makedirs(BUILD, exist_ok=True)
+    write_jit_sources()
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         results = list(ex.map(lambda s: _compile(s, list(extra)), srcs))
