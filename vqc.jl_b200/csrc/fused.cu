@@ -1219,12 +1219,14 @@ static int jit_grid(int device, const void* k, const PassShape& ps) {
 
 template <int M, bool ADJ>
 static int launch_tile_jit(vqc_state h, const void* k, void* psi, void* lam, const DevPass* dp, const void* ds,
-                           const DevOp* dops, const void* pool, double* partials, int grid, const PassShape& ps) {
+                           const DevOp* dops, const void* pool, double* partials, int grid, const PassShape& ps,
+                           const void* host_pool) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t smem = pass_smem<float, M, ADJ>(ps);
   VQC_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
   ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward", (double)(ADJ ? 4 : 2) * h->size() * sizeof(float2));
-  void* args[] = {&psi, &lam, (void*)&dp, (void*)&ds, (void*)&dops, (void*)&pool, &partials};
+  // the last parameter is the pass's matrix pool by value (host copy)
+  void* args[] = {&psi, &lam, (void*)&dp, (void*)&ds, (void*)&dops, (void*)&pool, &partials, const_cast<void*>(host_pool)};
   VQC_CK(cudaLaunchKernel(k, dim3(grid), dim3(NT), args, smem, h->stream));
   return VQC_OK;
 }
@@ -1253,7 +1255,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
       for (size_t pi = 0; pi < passes.size(); ++pi)
         if (!locs[pi].standalone)
           srcs[pi] = jit_pass_source(M, ADJ, (const DevStageF*)(sp.buf.data() + locs[pi].stages),
-                                     locs[pi].shape.nstages, (const DevOp*)(sp.buf.data() + locs[pi].ops));
+                                     locs[pi].shape.nstages, (const DevOp*)(sp.buf.data() + locs[pi].ops),
+                                     locs[pi].shape.npool);
       jit_kernels(srcs, jk);
     }
   }
@@ -1305,7 +1308,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     const void* dpool = base + pool_off + locs[pi].pool_begin * sizeof(cplx<R>);
     if (jk[pi]) {
       if constexpr (std::is_same<R, float>::value)
-        if ((rc = launch_tile_jit<M, ADJ>(h, jk[pi], psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape)))
+        if ((rc = launch_tile_jit<M, ADJ>(h, jk[pi], psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape,
+                                          sp.buf.data() + pool_off + locs[pi].pool_begin * sizeof(float2))))
           return rc;
     } else if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape))) {
       return rc;

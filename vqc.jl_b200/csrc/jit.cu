@@ -21,6 +21,7 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -128,7 +129,7 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o) {
   if (type == kOpU1) {
     const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = (code >> 14) & 3;
     const int cb = rctl == 0 ? -1 : rctl - 1;
-    os << "      const u64* c = reinterpret_cast<const u64*>(x.pool + op->mat);\n";
+    os << "      const u64* c = coef.c + " << op.mat << ";\n";
     if (ctl) os << "      const bool run = (tthr & op->cmask) == op->cval;\n";
     if (acc) os << "      float s8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};\n";
     os << "      " << (ctl ? "if (run) " : "") << "{\n";
@@ -147,9 +148,11 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o) {
   } else if (type == kOpU2) {
     const int ja = (code >> 4) & 3, jb = (code >> 6) & 3;
     if (ctl) os << "      if ((tthr & op->cmask) == op->cval)\n";
-    os << "      u2_op<" << ja << ", " << jb << ", ADJ>(v, w, x.pool + op->mat, (uint32_t)op->rmask);\n";
+    os << "      u2_op<" << ja << ", " << jb << ", ADJ>(v, w, reinterpret_cast<const float2*>(coef.c + " << op.mat
+       << "), (uint32_t)op->rmask);\n";
   } else if (type == kOpDiag) {
-    os << "      diag_op<ADJ>(v, w, op, x.pool + op->mat, tthr, S->dep, x.base);\n";
+    os << "      diag_op<ADJ>(v, w, op, reinterpret_cast<const float2*>(coef.c + " << op.mat
+       << "), tthr, S->dep, x.base);\n";
   } else {
     os << "      float s8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};\n"
        << "      accd_op(v, w, op, tthr, S->dep, x.base, s8);\n"
@@ -172,19 +175,23 @@ bool jit_available() { return nvrtc().ok; }
 
 int jit_min_blocks(bool adj) { return adj ? env_int("VQC_JIT_MINB_ADJ", 2) : env_int("VQC_JIT_MINB_FWD", 3); }
 
-std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops) {
+std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool) {
+  if (npool > kJitMaxCoef) return std::string();  // beyond the kernel-parameter space: interpreter
   std::ostringstream os;
   const int NT = 1 << (M - kRegBits);
+  // the pass's matrix pool travels as a kernel parameter (constant bank,
+  // read uniformly by the whole grid) instead of through shared memory
   os << "#include \"tile_f32.cuh\"\n"
      << "using namespace vqc;\nusing namespace vqc::f32t;\n"
+     << "struct Coef { unsigned long long c[" << std::max(npool, 2) << "]; };\n"
      << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj) << ")\n"
      << "vqc_pass(float2* psi, float2* lam, const DevPass* pass, const DevStageF* stages, const DevOp* ops,\n"
-     << "         const float2* pool, double* partials) {\n"
+     << "         const float2* pool, double* partials, const __grid_constant__ Coef coef) {\n"
      << "  constexpr int M = " << M << ";\n  constexpr bool ADJ = " << (adj ? "true" : "false") << ";\n"
      << "  constexpr int NW = TileCtx<M, ADJ>::NW;\n"
      << "  __shared__ DevPass P;\n  __shared__ uint64_t s_inc, s_base0;\n"
      << "  TileCtx<M, ADJ> x;\n"
-     << "  tile_setup<M, ADJ>(x, psi, lam, pass, stages, ops, pool, gridDim.x, P, s_inc, s_base0);\n"
+     << "  tile_setup<M, ADJ>(x, psi, lam, pass, stages, ops, pool, gridDim.x, P, s_inc, s_base0, false);\n"
      << "  Pk v[8], w[8];\n"
      << "  for (int it = 0; it < x.ntiles_here; ++it) {\n";
   for (int s = 0; s < nst; ++s) {

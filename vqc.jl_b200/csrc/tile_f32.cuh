@@ -311,36 +311,31 @@ __device__ __forceinline__ void pack_lane(const u64 (&c)[4], float (&s)[8]) {
   s[4] = hi(c[2]), s[5] = hi(c[3]), s[6] = hi(c[0]), s[7] = hi(c[1]);
 }
 
-// Warp reduce-scatter of 8 doubles: lane L with L % 4 == 0 ends with the warp
-// total of value L / 4.
-__device__ __forceinline__ double warp_reduce8d(const double (&x)[8]) {
-  const int lane = threadIdx.x & 31;
-  double y[4], z[2];
+// Thread partials -> the warp's slot row in shared memory.  A warp
+// reduce-scatter of the 8 values: the first two levels (lanes 16 and 8
+// apart) in FP32, so each partial then sums at most 32 products; the last
+// three levels and everything after them (warps, CTAs, the grid) in FP64.
+// Afterwards lane L with L % 4 == 0 holds the warp total of value L / 4.
+// Every lane of the warp must call it.
+__device__ __forceinline__ void flush8(const float (&s)[8], double* sacc, int slot, int nwarps) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float y[4], z[2];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const double keep = b4 ? x[i + 4] : x[i], send = b4 ? x[i] : x[i + 4];
+    const float keep = b4 ? s[i + 4] : s[i], send = b4 ? s[i] : s[i + 4];
     y[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
   }
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
-    const double keep = b3 ? y[i + 2] : y[i], send = b3 ? y[i] : y[i + 2];
+    const float keep = b3 ? y[i + 2] : y[i], send = b3 ? y[i] : y[i + 2];
     z[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
   }
-  double u = (b2 ? z[1] : z[0]) + __shfl_xor_sync(0xffffffffu, b2 ? z[0] : z[1], 4);
+  const double z0 = z[0], z1 = z[1];
+  double u = (b2 ? z1 : z0) + __shfl_xor_sync(0xffffffffu, b2 ? z0 : z1, 4);
   u += __shfl_xor_sync(0xffffffffu, u, 2);
   u += __shfl_xor_sync(0xffffffffu, u, 1);
-  return u;
-}
-// Thread partials (FP32) -> FP64 warp sums -> the warp's slot row in shared
-// memory.  Every lane of the warp must call it.
-__device__ __forceinline__ void flush8(const float (&s)[8], double* sacc, int slot, int nwarps) {
-  double x[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) x[i] = (double)s[i];
-  const double u = warp_reduce8d(x);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if ((lane & 3) == 0) sacc[((size_t)slot * nwarps + warp) * 8 + (lane >> 2)] += u;
+  if ((lane & 3) == 0) sacc[((unsigned long long)slot * nwarps + warp) * 8 + (lane >> 2)] += u;
 }
 
 template <int TB, int CB, int KIND>
@@ -575,7 +570,7 @@ struct TileCtx {
 template <int M, bool ADJ>
 __device__ __forceinline__ void tile_setup(TileCtx<M, ADJ>& x, float2* psi, float2* lam, const DevPass* pass,
                                            const DevStageF* stages, const DevOp* ops, const float2* pool, int ncta,
-                                           DevPass& P, uint64_t& s_inc, uint64_t& s_base0) {
+                                           DevPass& P, uint64_t& s_inc, uint64_t& s_base0, bool stage_pool = true) {
   constexpr int NT = TileCtx<M, ADJ>::NT, NW = TileCtx<M, ADJ>::NW, NPAIR = TileCtx<M, ADJ>::NPAIR;
   extern __shared__ __align__(16) unsigned char smem[];
   if (threadIdx.x == 0) P = *pass;
@@ -599,7 +594,8 @@ __device__ __forceinline__ void tile_setup(TileCtx<M, ADJ>& x, float2* psi, floa
     int4* d3 = reinterpret_cast<int4*>(dst + b1 + b2);
     for (unsigned i = threadIdx.x; i < b1 / 16; i += NT) d1[i] = __ldg(s1 + i);
     for (unsigned i = threadIdx.x; i < b2 / 16; i += NT) d2[i] = __ldg(s2 + i);
-    for (unsigned i = threadIdx.x; i < (b3 + 15) / 16; i += NT) d3[i] = __ldg(s3 + i);
+    if (stage_pool)
+      for (unsigned i = threadIdx.x; i < (b3 + 15) / 16; i += NT) d3[i] = __ldg(s3 + i);
     x.stages = reinterpret_cast<const DevStageF*>(dst) - P.stage_begin;
     x.ops = reinterpret_cast<const DevOp*>(dst + b1);
     x.pool = reinterpret_cast<const float2*>(dst + b1 + b2);

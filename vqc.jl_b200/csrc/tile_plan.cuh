@@ -140,7 +140,10 @@ struct ReqPlan {
 int jit_mode();        // 0 off, 1 on, 2 auto (VQC_JIT)
 bool jit_available();  // NVRTC could be loaded
 int jit_min_blocks(bool adj);
-std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops);
+// Source of a pass's kernel ("" when the pass is not compiled: its matrix
+// pool, passed as a kernel parameter, would exceed kJitMaxCoef entries).
+constexpr int kJitMaxCoef = 3800;
+std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops, int npool);
 // Kernels for the given pass sources (nullptr for an empty source or a failed compile).
 int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out);
 
