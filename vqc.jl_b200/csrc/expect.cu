@@ -97,6 +97,118 @@ __global__ void __launch_bounds__(kRedThreads)
   if (ACC) grid_reduce<2>(acc, s, res);
 }
 
+// Four consecutive outputs per thread, i = 4k + a (a = 0..3).  The partners
+// of group x are the four amplitudes at 4k ^ (x & ~3), permuted by x & 3.
+// A term's sign (-1)^{|j & z|} splits into its high bits (the same for the
+// four partners) and its low-bit class z & 3, so every term is evaluated
+// once per four outputs into class sums F[cls]; a 4-point Walsh-Hadamard
+// transform of F gives the group's phase at each partner's low bits b:
+//   f(b) = sum_cls (-1)^{|b & cls|} F[cls].
+// Terms arrive sorted by class, group g's class c in [cs[g][c], cs[g][c+1]).
+// SEP: separate coefficients d for the written operator (complex Pauli
+// coefficients with the Hermitian part requested); otherwise the written
+// operator is dfac * (the expectation operator).
+struct DevGroup4 {
+  uint64_t x;
+  int cs[5];
+  int pad;
+};
+
+template <int AX>
+__device__ __forceinline__ void pauli4_add(double2 (&hv)[4], const double2 (&W)[4], const double2 (&kv)[4]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) hv[a] = cfma(W[a ^ AX], kv[a ^ AX], hv[a]);
+}
+__device__ __forceinline__ void pauli4_wh(const double2 (&F)[4], double2 (&W)[4]) {
+  const double2 s01 = make_double2(F[0].x + F[1].x, F[0].y + F[1].y), d01 = make_double2(F[0].x - F[1].x, F[0].y - F[1].y);
+  const double2 s23 = make_double2(F[2].x + F[3].x, F[2].y + F[3].y), d23 = make_double2(F[2].x - F[3].x, F[2].y - F[3].y);
+  W[0] = make_double2(s01.x + s23.x, s01.y + s23.y);
+  W[1] = make_double2(d01.x + d23.x, d01.y + d23.y);
+  W[2] = make_double2(s01.x - s23.x, s01.y - s23.y);
+  W[3] = make_double2(d01.x - d23.x, d01.y - d23.y);
+}
+template <class R>
+__device__ __forceinline__ void load4(const cplx<R>* p, double2 (&kv)[4]) {
+  if constexpr (sizeof(R) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 2);
+    kv[0] = make_double2(a.x, a.y), kv[1] = make_double2(a.z, a.w);
+    kv[2] = make_double2(b.x, b.y), kv[3] = make_double2(b.z, b.w);
+  } else {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) kv[b] = to_d2(p[b]);
+  }
+}
+
+template <class R, bool WRITE, bool ACC, bool SEP>
+__global__ void __launch_bounds__(kRedThreads)
+    k_pauli4(const cplx<R>* __restrict__ bra, const cplx<R>* __restrict__ ket, cplx<R>* __restrict__ out, int64_t N,
+             const DevGroup4* __restrict__ groups, int ng, const DevTerm* __restrict__ terms, int nt, double dfac,
+             Scratch s, double* res) {
+  extern __shared__ unsigned char smem[];
+  DevGroup4* sg = reinterpret_cast<DevGroup4*>(smem);
+  DevTerm* st = reinterpret_cast<DevTerm*>(smem + sizeof(DevGroup4) * ng);
+  for (int i = threadIdx.x; i < ng; i += blockDim.x) sg[i] = groups[i];
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) st[i] = terms[i];
+  __syncthreads();
+  double acc[2] = {0, 0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, nq4 = N >> 2;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nq4; k += stride) {
+    const int64_t i0 = k << 2;
+    double2 hv[4], ov[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) hv[a] = ov[a] = make_double2(0, 0);
+    for (int gi = 0; gi < ng; ++gi) {
+      const DevGroup4& g = sg[gi];
+      const int64_t jb = i0 ^ (int64_t)(g.x & ~3ull);
+      double2 kv[4];
+      load4<R>(ket + jb, kv);
+      double2 F[4], Fd[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        F[c] = Fd[c] = make_double2(0, 0);
+        for (int q = g.cs[c]; q < g.cs[c + 1]; ++q) {
+          const uint64_t m = (uint64_t)jb & st[q].z;
+          const bool odd = (__popc((unsigned)m ^ (unsigned)(m >> 32)) & 1) != 0;
+          const double2 cc = st[q].c;
+          F[c].x += odd ? -cc.x : cc.x;
+          F[c].y += odd ? -cc.y : cc.y;
+          if (SEP) {
+            const double2 dd = st[q].d;
+            Fd[c].x += odd ? -dd.x : dd.x;
+            Fd[c].y += odd ? -dd.y : dd.y;
+          }
+        }
+      }
+      double2 W[4], Wd[4];
+      pauli4_wh(F, W);
+      if (SEP) pauli4_wh(Fd, Wd);
+      switch ((int)(g.x & 3)) {
+        case 0: pauli4_add<0>(hv, W, kv); if (SEP) pauli4_add<0>(ov, Wd, kv); break;
+        case 1: pauli4_add<1>(hv, W, kv); if (SEP) pauli4_add<1>(ov, Wd, kv); break;
+        case 2: pauli4_add<2>(hv, W, kv); if (SEP) pauli4_add<2>(ov, Wd, kv); break;
+        default: pauli4_add<3>(hv, W, kv); if (SEP) pauli4_add<3>(ov, Wd, kv); break;
+      }
+    }
+    if (WRITE) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const double2 o = SEP ? ov[a] : make_double2(dfac * hv[a].x, dfac * hv[a].y);
+        out[i0 + a] = mkc<R>((R)o.x, (R)o.y);
+      }
+    }
+    if (ACC) {
+      double2 b[4];
+      load4<R>(bra + i0, b);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        acc[0] = fma(b[a].x, hv[a].x, fma(b[a].y, hv[a].y, acc[0]));
+        acc[1] = fma(b[a].x, hv[a].y, fma(-b[a].y, hv[a].x, acc[1]));
+      }
+    }
+  }
+  if (ACC) grid_reduce<2>(acc, s, res);
+}
+
 template <class R>
 __global__ void k_axpy(cplx<R>* y, const cplx<R>* x, int64_t N) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
@@ -132,9 +244,33 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
       if (write && first) VQC_CK(cudaMemsetAsync(out, 0, h->size() * h->amp_bytes(), h->stream));
       break;
     }
-    const size_t gb = sizeof(DevGroup) * p.groups.size(), tb = sizeof(DevTerm) * p.terms.size();
+    // quad kernel (n >= 2): terms of each group sorted by their low-bit class
+    const bool quad = h->nq >= 2;
+    std::vector<DevGroup4> g4;
+    bool sep = false;
+    if (quad) {
+      std::vector<DevTerm> sorted;
+      for (const DevGroup& g : p.groups) {
+        DevGroup4 q{};
+        q.x = g.x;
+        for (int c = 0; c < 4; ++c) {
+          q.cs[c] = (int)sorted.size();
+          for (int t = g.start; t < g.start + g.count; ++t)
+            if ((int)(p.terms[t].z & 3) == c) sorted.push_back(p.terms[t]);
+        }
+        q.cs[4] = (int)sorted.size();
+        g4.push_back(q);
+      }
+      p.terms.swap(sorted);
+      // one coefficient set unless the written operator is not a multiple of the expectation's
+      const double f = hermitian_part ? 2.0 : 1.0;
+      for (const DevTerm& t : p.terms)
+        if (t.d.x != f * t.c.x || t.d.y != f * t.c.y) sep = true;
+    }
+    const size_t gb = quad ? sizeof(DevGroup4) * g4.size() : sizeof(DevGroup) * p.groups.size(),
+                 tb = sizeof(DevTerm) * p.terms.size();
     std::vector<unsigned char> buf(gb + tb);
-    std::memcpy(buf.data(), p.groups.data(), gb);
+    std::memcpy(buf.data(), quad ? (const void*)g4.data() : (const void*)p.groups.data(), gb);
     std::memcpy(buf.data() + gb, p.terms.data(), tb);
     if ((rc = upload_ops(h, buf.data(), buf.size()))) return rc;
     const DevGroup* dg = (const DevGroup*)h->opbuf;
@@ -153,11 +289,21 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
                    (double)h->size() * h->amp_bytes() * (1 + (write ? 1 : 0) + (acc && bra != ket ? 1 : 0)));
 #define VQC_PAULI_LAUNCH(R)                                                                                      \
   do {                                                                                                           \
-    auto kfun = write ? (acc ? k_pauli<R, true, true> : k_pauli<R, true, false>)                                 \
-                      : k_pauli<R, false, true>;                                                                 \
-    if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    kfun<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,     \
-                                                  h->size(), dg, ng, dt, nt, h->scr, h->scr.result);             \
+    if (quad) {                                                                                                  \
+      auto kfun = write ? (acc ? (sep ? k_pauli4<R, true, true, true> : k_pauli4<R, true, true, false>)          \
+                               : (sep ? k_pauli4<R, true, false, true> : k_pauli4<R, true, false, false>))       \
+                        : k_pauli4<R, false, true, false>;                                                       \
+      if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+      kfun<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,   \
+                                                    h->size(), (const DevGroup4*)h->opbuf, ng, dt, nt,           \
+                                                    hermitian_part ? 2.0 : 1.0, h->scr, h->scr.result);          \
+    } else {                                                                                                     \
+      auto kfun = write ? (acc ? k_pauli<R, true, true> : k_pauli<R, true, false>)                               \
+                        : k_pauli<R, false, true>;                                                               \
+      if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+      kfun<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,   \
+                                                    h->size(), dg, ng, dt, nt, h->scr, h->scr.result);           \
+    }                                                                                                            \
   } while (0)
     if (h->dtype == VQC_C64)
       VQC_PAULI_LAUNCH(float);

@@ -815,6 +815,7 @@ static void plan_stages(PlanPass& p, int M, int dtype) {
         found = true;
       }
     }
+    if (!found) prof_note("plan_stages_bank_conflicted", 1);
     st.rs = best;
     p.stages.push_back(st);
     pending = rest;
