@@ -26,6 +26,7 @@
 // the warp, the CTA and the grid, in a fixed order); the host contracts A
 // with D_j = B^dagger dB/dtheta_j of each parameter j of the (merged) block.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <type_traits>
@@ -622,7 +623,8 @@ struct TileConfig {
 static TileConfig tile_config(int dtype, int n) {
   // 2^12 FP32 or 2^11 FP64 amplitudes per tile (32 KiB per state), smaller
   // tiles for smaller states; the lowest 4 (FP32) / 3 (FP64) qubits are always
-  // tile qubits so that a tile is made of 128-byte runs
+  // tile qubits so that a tile is made of 128-byte runs (11-qubit FP32 tiles
+  // for the reverse sweep measured slower: more passes at the same pass cost)
   const int M = std::min(dtype == VQC_C64 ? 12 : 11, n);
   return {M, std::min(dtype == VQC_C64 ? 4 : 3, M)};
 }

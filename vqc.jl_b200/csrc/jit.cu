@@ -173,7 +173,12 @@ int jit_mode() {
 
 bool jit_available() { return nvrtc().ok; }
 
-int jit_min_blocks(bool adj) { return adj ? env_int("VQC_JIT_MINB_ADJ", 2) : env_int("VQC_JIT_MINB_FWD", 3); }
+// Resident CTAs per SM the compiled kernels' registers are budgeted for:
+// 768 threads for forward passes, 512 for the reverse sweep.
+int jit_min_blocks(bool adj, int M) {
+  const int nt = 1 << (M - kRegBits);
+  return adj ? env_int("VQC_JIT_MINB_ADJ", 512 / nt) : env_int("VQC_JIT_MINB_FWD", 768 / nt);
+}
 
 std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool) {
   if (npool > kJitMaxCoef) return std::string();  // beyond the kernel-parameter space: interpreter
@@ -184,7 +189,7 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
   os << "#include \"tile_f32.cuh\"\n"
      << "using namespace vqc;\nusing namespace vqc::f32t;\n"
      << "struct Coef { unsigned long long c[" << std::max(npool, 2) << "]; };\n"
-     << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj) << ")\n"
+     << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M) << ")\n"
      << "vqc_pass(float2* psi, float2* lam, const DevPass* pass, const DevStageF* stages, const DevOp* ops,\n"
      << "         const float2* pool, double* partials, const __grid_constant__ Coef coef) {\n"
      << "  constexpr int M = " << M << ";\n  constexpr bool ADJ = " << (adj ? "true" : "false") << ";\n"
@@ -194,12 +199,25 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
      << "  tile_setup<M, ADJ>(x, psi, lam, pass, stages, ops, pool, gridDim.x, P, s_inc, s_base0, false);\n"
      << "  Pk v[8], w[8];\n"
      << "  for (int it = 0; it < x.ntiles_here; ++it) {\n";
+  const bool bake = env_int("VQC_JIT_BAKE", 1) != 0;
   for (int s = 0; s < nst; ++s) {
-    os << "  {\n    const DevStageF* S = x.stages + " << s << ";\n"
-       << "    stage_load<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w);\n"
-       << "    const uint32_t tthr = S->thr[0][x.tlo] | S->thr[1][x.thi];\n    (void)tthr;\n";
+    os << "  {\n    const DevStageF* S = x.stages + " << s << ";\n";
+    if (bake) {
+      // the stage's pair offsets as constants (they depend on the pass's qubits)
+      os << "    constexpr uint32_t swm[8] = {";
+      for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[s].swm[m] << "u";
+      os << "};\n    constexpr int64_t gdep[8] = {";
+      for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[s].gdep[m] << "ll";
+      os << "};\n    stage_load_k<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w, swm, gdep);\n";
+    } else {
+      os << "    stage_load<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w);\n";
+    }
+    os << "    const uint32_t tthr = S->thr[0][x.tlo] | S->thr[1][x.thi];\n    (void)tthr;\n";
     for (int o = st[s].op_begin; o < st[s].op_end; ++o) emit_op(os, ops[o], o);
-    os << "    stage_store<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w);\n  }\n";
+    if (bake)
+      os << "    stage_store_k<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w, swm, gdep);\n  }\n";
+    else
+      os << "    stage_store<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w);\n  }\n";
   }
   os << "    tile_next<M, ADJ>(x, s_inc);\n  }\n  tile_finish<M, ADJ>(x, partials);\n  (void)NW;\n}\n";
   return os.str();

@@ -683,6 +683,66 @@ __device__ __forceinline__ void stage_store(const TileCtx<M, ADJ>& x, const DevS
   }
   __syncthreads();  // also orders this tile's last shared reads before the next tile's writes
 }
+// The same with the stage's pair offsets as compile-time constants (the
+// compiled pass kernels): no dependent descriptor loads before the data.
+template <int M, bool ADJ>
+__device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ>& x, const DevStageF* S, bool first, Pk (&v)[8],
+                                             Pk (&w)[8], const uint32_t (&swm)[8], const int64_t (&gdep)[8]) {
+  if (first) {
+    const int64_t g0 = (int64_t)x.base + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int64_t gi = g0 + gdep[m];
+      const float4 t = *reinterpret_cast<const float4*>(x.psi + gi);
+      v[m].r = mk(t.x, t.z);
+      v[m].i = mk(t.y, t.w);
+      if (ADJ) {
+        const float4 u = *reinterpret_cast<const float4*>(x.lam + gi);
+        w[m].r = mk(u.x, u.z);
+        w[m].i = mk(u.y, u.w);
+      }
+    }
+  } else {
+    const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint32_t a = sw ^ swm[m];
+      const ulonglong2 t = x.sp[a];
+      v[m].r = t.x;
+      v[m].i = t.y;
+      if (ADJ) {
+        const ulonglong2 u = x.sl[a];
+        w[m].r = u.x;
+        w[m].i = u.y;
+      }
+    }
+  }
+}
+template <int M, bool ADJ>
+__device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const DevStageF* S, bool last,
+                                              const Pk (&v)[8], const Pk (&w)[8], const uint32_t (&swm)[8],
+                                              const int64_t (&gdep)[8]) {
+  if (last) {
+    const int64_t g0 = (int64_t)x.base + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int64_t gi = g0 + gdep[m];
+      *reinterpret_cast<float4*>(x.psi + gi) = make_float4(lo(v[m].r), lo(v[m].i), hi(v[m].r), hi(v[m].i));
+      if (ADJ)
+        *reinterpret_cast<float4*>(x.lam + gi) = make_float4(lo(w[m].r), lo(w[m].i), hi(w[m].r), hi(w[m].i));
+    }
+  } else {
+    const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint32_t a = sw ^ swm[m];
+      x.sp[a] = make_ulonglong2(v[m].r, v[m].i);
+      if (ADJ) x.sl[a] = make_ulonglong2(w[m].r, w[m].i);
+    }
+  }
+  __syncthreads();
+}
+
 template <int M, bool ADJ>
 __device__ __forceinline__ void tile_next(TileCtx<M, ADJ>& x, uint64_t s_inc) {
   x.base = ((x.base | ~x.P->nontile_mask) + s_inc) & x.P->nontile_mask;

@@ -139,7 +139,7 @@ struct ReqPlan {
 // Run-time specialised FP32 tile kernels (jit.cu).
 int jit_mode();        // 0 off, 1 on, 2 auto (VQC_JIT)
 bool jit_available();  // NVRTC could be loaded
-int jit_min_blocks(bool adj);
+int jit_min_blocks(bool adj, int M);
 // Source of a pass's kernel ("" when the pass is not compiled: its matrix
 // pool, passed as a kernel parameter, would exceed kJitMaxCoef entries).
 constexpr int kJitMaxCoef = 3800;
