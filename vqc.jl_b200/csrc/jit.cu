@@ -212,6 +212,8 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
     } else {
       os << "    stage_load<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w);\n";
     }
+    if (s == 0 && bake && env_int("VQC_JIT_L2PF", 1))
+      os << "    if (it + 1 < x.ntiles_here) prefetch_next_l2<M, ADJ>(x, S, s_inc, gdep);\n";
     os << "    const uint32_t tthr = S->thr[0][x.tlo] | S->thr[1][x.thi];\n    (void)tthr;\n";
     for (int o = st[s].op_begin; o < st[s].op_end; ++o) emit_op(os, ops[o], o);
     if (bake)

@@ -743,6 +743,20 @@ __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const De
   __syncthreads();
 }
 
+// L2 prefetch of the next tile's first-stage pairs (no shared memory, no
+// registers held): the next tile's loads then come from L2.
+template <int M, bool ADJ>
+__device__ __forceinline__ void prefetch_next_l2(const TileCtx<M, ADJ>& x, const DevStageF* S, uint64_t s_inc,
+                                                 const int64_t (&gdep)[8]) {
+  const uint64_t next = ((x.base | ~x.P->nontile_mask) + s_inc) & x.P->nontile_mask;
+  const int64_t g0 = (int64_t)next + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(x.psi + g0 + gdep[m]));
+    if (ADJ) asm volatile("prefetch.global.L2 [%0];" ::"l"(x.lam + g0 + gdep[m]));
+  }
+}
+
 template <int M, bool ADJ>
 __device__ __forceinline__ void tile_next(TileCtx<M, ADJ>& x, uint64_t s_inc) {
   x.base = ((x.base | ~x.P->nontile_mask) + s_inc) & x.P->nontile_mask;
