@@ -1254,13 +1254,12 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   std::vector<const void*> jk(passes.size(), nullptr);
   if constexpr (std::is_same<R, float>::value) {
     if (use_jit(h)) {
-      std::vector<std::string> srcs(passes.size());
+      std::vector<JitPassRef> refs(passes.size());
       for (size_t pi = 0; pi < passes.size(); ++pi)
         if (!locs[pi].standalone)
-          srcs[pi] = jit_pass_source(M, ADJ, (const DevStageF*)(sp.buf.data() + locs[pi].stages),
-                                     locs[pi].shape.nstages, (const DevOp*)(sp.buf.data() + locs[pi].ops),
-                                     locs[pi].shape.npool);
-      jit_kernels(srcs, jk);
+          refs[pi] = JitPassRef{(const DevStageF*)(sp.buf.data() + locs[pi].stages), locs[pi].shape.nstages,
+                                (const DevOp*)(sp.buf.data() + locs[pi].ops), locs[pi].shape.npool};
+      jit_pass_kernels(M, ADJ, refs, jk);
     }
   }
   std::vector<int> grids(passes.size(), 0);

@@ -292,4 +292,81 @@ int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& 
   return VQC_OK;
 }
 
+// Kernels of many passes by structure: a 128-bit hash of everything the
+// generated source depends on keys a second cache, so a pass seen before
+// costs a hash, not a source text.
+namespace {
+struct Hash128 {
+  uint64_t a = 1469598103934665603ull, b = 0x9e3779b97f4a7c15ull;
+  void add(const void* p, size_t n) {
+    const unsigned char* c = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) {
+      a = (a ^ c[i]) * 1099511628211ull;
+      b = (b + c[i]) * 0xff51afd7ed558ccdull;
+      b ^= b >> 29;
+    }
+  }
+  template <class T>
+  void val(const T& v) {
+    add(&v, sizeof(v));
+  }
+};
+std::map<std::pair<uint64_t, uint64_t>, const void*>& hcache() {
+  static std::map<std::pair<uint64_t, uint64_t>, const void*> c;
+  return c;
+}
+}  // namespace
+
+int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out) {
+  out.assign(refs.size(), nullptr);
+  if (!jit_available()) return VQC_OK;
+  const int flags[4] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M), M};
+  std::vector<std::pair<uint64_t, uint64_t>> keys(refs.size());
+  std::vector<size_t> miss;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (size_t i = 0; i < refs.size(); ++i) {
+      const JitPassRef& r = refs[i];
+      if (!r.stages || r.npool > kJitMaxCoef) continue;
+      Hash128 h;
+      h.add(flags, sizeof(flags));
+      h.val(adj);
+      h.val(r.nstages);
+      h.val(r.npool);
+      for (int s = 0; s < r.nstages; ++s) {
+        const DevStageF& st = r.stages[s];
+        h.add(st.swm, sizeof(st.swm));
+        h.add(st.gdep, sizeof(st.gdep));
+        h.val(st.op_begin);
+        h.val(st.op_end);
+        for (int o = st.op_begin; o < st.op_end; ++o) {
+          h.val(r.ops[o].code);
+          h.val(r.ops[o].mat);
+        }
+      }
+      keys[i] = {h.a, h.b};
+      auto it = hcache().find(keys[i]);
+      if (it != hcache().end())
+        out[i] = it->second;
+      else
+        miss.push_back(i);
+    }
+  }
+  if (miss.empty()) return VQC_OK;
+  std::vector<std::string> srcs(miss.size());
+  for (size_t k = 0; k < miss.size(); ++k) {
+    const JitPassRef& r = refs[miss[k]];
+    srcs[k] = jit_pass_source(M, adj, r.stages, r.nstages, r.ops, r.npool);
+  }
+  std::vector<const void*> ks;
+  int rc = jit_kernels(srcs, ks);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (size_t k = 0; k < miss.size(); ++k) {
+    out[miss[k]] = ks[k];
+    hcache()[keys[miss[k]]] = ks[k];  // (nullptr: compiled and failed; the interpreter runs it)
+  }
+  return VQC_OK;
+}
+
 }  // namespace vqc

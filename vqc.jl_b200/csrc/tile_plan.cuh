@@ -146,6 +146,15 @@ constexpr int kJitMaxCoef = 3800;
 std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops, int npool);
 // Kernels for the given pass sources (nullptr for an empty source or a failed compile).
 int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out);
+// A serialised pass for jit_pass_kernels (stages == nullptr: not a tile pass).
+struct JitPassRef {
+  const DevStageF* stages = nullptr;
+  int nstages = 0;
+  const DevOp* ops = nullptr;
+  int npool = 0;
+};
+// Kernels for many passes, looked up by a hash of their structure first.
+int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out);
 
 int serve_build_plan(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
                      const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp);

@@ -4,6 +4,8 @@ QCircuit is a gate list (QuantumCircuits.jl's QCircuit, iterated by
 applygates/generic/generic.jl:26-31).  `pack` turns it into the vqc_gate /
 vqc_param arrays and the FP64 matrix pool of include/vqc_b200.h.
 """
+import ctypes
+
 import numpy as np
 
 from . import _lib
@@ -20,6 +22,7 @@ class QCircuit:
         if not isinstance(g, Gate):
             raise TypeError("QCircuit holds Gate objects")
         self.gates.append(g)
+        self._packed = None
         return self
 
     append = push
@@ -54,38 +57,76 @@ class QCircuit:
         return apply(self, state.copy())
 
 
+_GATE_DT = np.dtype([("nq", "<i4"), ("pos", "<i4", (5,)), ("mat", "<i8")], align=True)
+_PARAM_DT = np.dtype([("gate", "<i4"), ("kind", "<i4"), ("dmat", "<i8")], align=True)
+assert _GATE_DT.itemsize == ctypes.sizeof(_lib.Gate_t) and _PARAM_DT.itemsize == ctypes.sizeof(_lib.Param_t)
+
+
+def _gate_pack(g):
+    """Per-gate packing (0-based padded positions, FP64 matrix and derivative
+    matrices flattened re/im), computed once per Gate object: gates are
+    values, not changed after construction."""
+    pk = getattr(g, "_pk", None)
+    if pk is None:
+        pos = tuple(p - 1 for p in g.positions) + (0,) * (5 - g.nqubits)
+        mat = np.ascontiguousarray(g.mat, dtype=np.complex128).view(np.float64).ravel()
+        ders = tuple(np.ascontiguousarray(d, dtype=np.complex128).view(np.float64).ravel() for d in g.derivatives())
+        pk = g._pk = (g.nqubits, pos, mat, ders)
+    return pk
+
+
 class Packed:
-    """ctypes arrays for one circuit: gates, matrix pool, parameters."""
+    """ctypes arrays for one circuit: gates, matrix pool, parameters.
+
+    Built with numpy (the C structs' layouts as structured dtypes) and cached
+    on the QCircuit for as long as it holds the same gate objects, so a
+    circuit evaluated repeatedly (an optimisation loop) is packed once."""
+
+    def __new__(cls, circuit, with_params=True):
+        cache = getattr(circuit, "_packed", None) if isinstance(circuit, QCircuit) else None
+        gates = list(circuit)
+        if cache is not None:
+            key_gates, wp, packed = cache
+            if wp == with_params and len(key_gates) == len(gates) and all(a is b for a, b in zip(key_gates, gates)):
+                return packed
+        self = super().__new__(cls)
+        self._build(gates, with_params)
+        if isinstance(circuit, QCircuit):
+            circuit._packed = (gates, with_params, self)
+        return self
 
     def __init__(self, circuit, with_params=True):
-        gates = list(circuit)
+        pass
+
+    def _build(self, gates, with_params):
         ng = len(gates)
-        self.gates = (_lib.Gate_t * max(ng, 1))()
-        chunks, off = [], 0
-        params = []
-        for i, g in enumerate(gates):
-            k = g.nqubits
-            t = self.gates[i]
-            t.nq = k
-            for b in range(k):
-                t.pos[b] = g.positions[b] - 1  # 1-based -> 0-based
-            t.mat = off
-            m = np.ascontiguousarray(g.mat, dtype=np.complex128).view(np.float64).ravel()
-            chunks.append(m)
-            off += m.size
+        pks = [_gate_pack(g) for g in gates]
+        chunks, offs, params = [], [], []
+        off = 0
+        for i, (k, pos, mat, ders) in enumerate(pks):
+            offs.append(off)
+            chunks.append(mat)
+            off += mat.size
             if with_params:
-                for dU in g.derivatives():
-                    d = np.ascontiguousarray(dU, dtype=np.complex128).view(np.float64).ravel()
+                for d in ders:
                     params.append((i, off))
                     chunks.append(d)
                     off += d.size
+        self._garr = np.zeros(max(ng, 1), _GATE_DT)
+        if ng:
+            self._garr["nq"][:ng] = [pk[0] for pk in pks]
+            self._garr["pos"][:ng] = [pk[1] for pk in pks]
+            self._garr["mat"][:ng] = offs
+        self._parr = np.zeros(max(len(params), 1), _PARAM_DT)
+        if params:
+            pa = np.asarray(params, dtype=np.int64)
+            self._parr["gate"][:len(params)] = pa[:, 0]
+            self._parr["dmat"][:len(params)] = pa[:, 1]
+        self.gates = (_lib.Gate_t * len(self._garr)).from_buffer(self._garr)
+        self.params = (_lib.Param_t * len(self._parr)).from_buffer(self._parr)
         self.mats = np.concatenate(chunks) if chunks else np.zeros(1)
         self.ngates = ng
         self.nparams = len(params)
-        self.params = (_lib.Param_t * max(len(params), 1))()
-        for j, (gi, o) in enumerate(params):
-            self.params[j].gate = gi
-            self.params[j].dmat = o
 
     def mats_ptr(self):
         return self.mats.ctypes.data_as(_lib._D)

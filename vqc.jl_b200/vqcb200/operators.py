@@ -135,12 +135,19 @@ class QubitsOperator:
         return [(x, z, c) for (x, z), c in acc.items() if c != 0]
 
     def packed(self):
-        """ctypes vqc_pauli array of the merged Pauli strings."""
+        """ctypes vqc_pauli array of the merged Pauli strings (cached while
+        the operator holds the same terms with the same coefficients)."""
+        key = [(t, t.coeff) for t in self.terms]
+        cache = getattr(self, "_packed", None)
+        if cache is not None and len(cache[0]) == len(key) and all(
+                a[0] is b[0] and a[1] == b[1] for a, b in zip(cache[0], key)):
+            return cache[1], cache[2]
         ps = self.pauli_strings()
         arr = (_lib.Pauli_t * max(len(ps), 1))()
         for i, (x, z, c) in enumerate(ps):
             arr[i].xmask, arr[i].zmask = x, z
             arr[i].coeff_re, arr[i].coeff_im = c.real, c.imag
+        self._packed = (key, arr, len(ps))
         return arr, len(ps)
 
     def is_hermitian(self):
