@@ -176,6 +176,17 @@ int vqc_dm_ptrace(vqc_state rho, int nsites, const int* sites, double* out);
 int vqc_dm_probs(vqc_state rho, double* out);
 /* tr(rho) (densitymatrix.jl:58), FP64 (re, im). */
 int vqc_dm_trace(vqc_state rho, double* out);
+/* apply!(::QuantumMap, ::DensityMatrix) (applygates/apply_qmaps.jl:5-14),
+ * apply_dagger! (:21-30), apply_inverse! (:36-45): rho <- sum_i K_i rho K_i^dagger
+ * for the nkraus Kraus operators K_i (2^k x 2^k, row-major, complex FP64
+ * interleaved, index bit b <-> pos[b], like gates), applied as the channel's
+ * supermatrix on (pos, pos + n) (apply_qmaps.jl:67-77).  mode 0 = apply,
+ * 1 = the supermatrix's adjoint, 2 = its inverse.  k = 1 or 2 (the
+ * supermatrix is a 2k-qubit gate; the reference's gate kernels stop at 5). */
+int vqc_dm_apply_channel(vqc_state rho, int k, const int* pos, int nkraus, const double* kraus, int mode);
+/* expectation(::QubitsOperator, ::DensityMatrix) = tr(H rho)
+ * (hamiltonian/expecs_dm/expecs_dm.jl:19-30), FP64 (re, im). */
+int vqc_dm_expect_pauli(vqc_state rho, const vqc_pauli* terms, int nterms, double* out);
 
 /* ---- allocation-free expectation (no counterpart in the reference) ------
  * For callers that cannot allocate device memory (a fixed arena handed over

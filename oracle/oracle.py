@@ -308,3 +308,32 @@ def dm_probs(rho, n):
 def dm_prob_zero(rho, n, q):
     """compute_probability_zero(rho, q) (measure.jl:69-81)."""
     return lib().or_dm_prob_zero_c128(_ptr(rho), n, q)
+
+
+def dm_apply_channel(rho, n, pos, kraus, mode=0, nthreads=1):
+    """apply!(::QuantumMap, rho) (apply_qmaps.jl:5-14, 67-77): the channel's
+    supermatrix sum_i kron(conj K_i, K_i) as a gate on (pos..., pos + n...)
+    of the vectorised rho; mode 1 its adjoint (apply_dagger!, :21-30,
+    79-86), mode 2 its inverse (apply_inverse!, :36-45)."""
+    S = sum(np.kron(np.asarray(K, dtype=np.complex128).conj(), np.asarray(K, dtype=np.complex128)) for K in kraus)
+    if mode == 1:
+        S = S.conj().T
+    elif mode == 2:
+        S = np.linalg.inv(S)
+    return apply_gate(rho, list(pos) + [p + n for p in pos], S, nthreads)
+
+
+def dm_expectation(terms, rho, n):
+    """expectation(H, rho) (expecs_dm.jl:19-30): sum over position keys of
+    tr(M_key rho_key), rho_key the reduced matrix of the key's qubits (the
+    blocks expec_dm_serial.jl sums); the empty key gives coeff * tr(rho)."""
+    r = 0j
+    for pos, M in group_by_key(terms).items():
+        if len(pos) == 0:
+            r += M[0, 0] * complex(np.sum(dm_probs(rho, n)))
+            continue
+        rest = [q for q in range(n) if q not in pos]
+        red = dm_ptrace(rho, n, rest) if rest else rho
+        d = 1 << len(pos)
+        r += complex(np.trace(M @ red.reshape(d, d, order="F")))
+    return r

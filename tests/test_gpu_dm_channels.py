@@ -1,0 +1,106 @@
+"""GPU parity of quantum channels and Pauli-sum expectations on density
+matrices (applygates/apply_qmaps.jl, hamiltonian/expecs_dm/expecs_dm.jl)
+against the oracle's restatement, and the oracle against dense NumPy
+(rho -> sum_i K_i rho K_i^dagger; tr(H rho)).
+Tolerances: helpers.tol (1e-12 FP64, 1e-5 FP32), scaled by the depth."""
+import numpy as np
+import pytest
+
+import vqcb200 as V
+from helpers import max_abs, rand_psi, tol
+from oracle import dense_np as D
+from oracle import gates_ref as GR
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+DTYPES = [np.complex128, np.complex64]
+
+
+def _kraus2(rng):
+    """A random 2-qubit channel: 3 Kraus operators, sum K^dagger K = I."""
+    A = [rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4)) for _ in range(3)]
+    S = sum(a.conj().T @ a for a in A)
+    w, U = np.linalg.eigh(S)
+    inv_sqrt = U @ np.diag(w ** -0.5) @ U.conj().T
+    return [a @ inv_sqrt for a in A]
+
+
+def _dense_channel(rho_vec, n, pos, kraus):
+    N = 1 << n
+    R = rho_vec.reshape(N, N, order="F")
+    out = sum(D.full_operator(n, pos, K) @ R @ D.full_operator(n, pos, K).conj().T for K in kraus)
+    return out.reshape(-1, order="F")
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_channels_on_density_matrix(dtype):
+    rng = np.random.default_rng(52)
+    n = 6
+    psi = rand_psi(rng, n)
+    rho = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
+    ref = O.density_matrix(psi)
+    maps = [V.Depolarizing(1, 0.1), V.AmplitudeDamping(4, 0.3), V.PhaseDamping(6, 0.25),
+            V.QuantumMap((2, 5), _kraus2(rng)), V.QuantumMap((6, 1), _kraus2(rng))]
+    for m in maps:
+        V.apply(m, rho)
+        O.dm_apply_channel(ref, n, [p - 1 for p in m.positions], m.kraus)
+    assert max_abs(rho.data(), ref) < tol(dtype) * 10
+    assert abs(rho.tr() - 1) < tol(dtype) * 10  # trace preserving
+    # adjoint and inverse of the supermatrix
+    m = V.QuantumMap((3, 2), _kraus2(rng))
+    V.apply_dagger(m, rho)
+    O.dm_apply_channel(ref, n, [2, 1], m.kraus, mode=1)
+    assert max_abs(rho.data(), ref) < tol(dtype) * 10
+    m = V.AmplitudeDamping(3, 0.2)
+    V.apply(m, rho)
+    V.apply_inverse(m, rho)
+    O.dm_apply_channel(ref, n, [2], m.kraus, mode=0)
+    O.dm_apply_channel(ref, n, [2], m.kraus, mode=2)
+    assert max_abs(rho.data(), ref) < tol(dtype) * 10
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_noisy_circuit_on_state(dtype):
+    """A circuit with channels (the reference's noisy_circuit: a layer of
+    Depolarizing after a variational circuit, test/check_noisy_grad.jl:3-9)
+    applied to a StateVector gives a DensityMatrix (apply_qmaps.jl:16)."""
+    rng = np.random.default_rng(53)
+    n = 5
+    gates = []
+    for q in range(1, n + 1):
+        gates.append(V.RyGate(q, float(rng.uniform(0, 6))))
+    for q in range(1, n):
+        gates.append(V.CNOTGate(q, q + 1))
+    c = V.QCircuit(gates + [V.Depolarizing(q, 0.1) for q in range(1, n + 1)] + [V.HGate(2)])
+    psi = rand_psi(rng, n)
+    out = V.apply(c, V.StateVector(psi.astype(dtype), dtype=dtype))
+    assert isinstance(out, V.DensityMatrix)
+    ref = O.density_matrix(psi)
+    for g in c:
+        pos = [p - 1 for p in g.positions]
+        if isinstance(g, V.QuantumMap):
+            O.dm_apply_channel(ref, n, pos, g.kraus)
+        else:
+            O.dm_apply_gate(ref, n, pos, g.mat)
+    assert max_abs(out.data(), ref) < tol(dtype) * 10
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("n", [3, 7, 10])
+def test_dm_pauli_expectation(dtype, n):
+    rng = np.random.default_rng(60 + n)
+    psi = rand_psi(rng, n)
+    rho = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
+    V.apply(V.Depolarizing(1, 0.2), rho)
+    ref = O.dm_apply_channel(O.density_matrix(psi), n, [0], V.Depolarizing(1, 0.2).kraus)
+    spec = [({1: "X", n: "Y"}, 0.36), ({1: "Z", 2: "Z"}, -0.8), ({2: "Y"}, 0.5 + 0.25j), ({n: "X", 1: "Z"}, 1.3),
+            ({}, 0.1)]
+    H = V.QubitsOperator(*[V.QubitsTerm(ops, coeff=c) for ops, c in spec])
+    terms = [O.make_term({q - 1: o for q, o in ops.items()}, c) for ops, c in spec]
+    got = V.expectation(H, rho)
+    want = O.dm_expectation(terms, ref, n)
+    assert abs(got - want) < tol(dtype) * 10 * max(1.0, abs(want))
+    # a pure state: tr(H |psi><psi|) = <psi|H|psi>
+    pure = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
+    sv = V.expectation(H, V.StateVector(psi.astype(dtype), dtype=dtype))
+    assert abs(V.expectation(H, pure) - sv) < tol(dtype) * 10 * max(1.0, abs(sv))

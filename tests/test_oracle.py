@@ -165,3 +165,36 @@ def test_oracle_rejects_bad_positions():
         O.apply_gate(v, [0, 0], np.eye(4))
     with pytest.raises(ValueError):
         O.apply_gate(v, [3], np.eye(2))
+
+
+def _kraus2_cpu(rng):
+    """A random 2-qubit channel: 3 Kraus operators, sum K^dagger K = I."""
+    A = [rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4)) for _ in range(3)]
+    S = sum(a.conj().T @ a for a in A)
+    w, U = np.linalg.eigh(S)
+    inv_sqrt = U @ np.diag(w ** -0.5) @ U.conj().T
+    return [a @ inv_sqrt for a in A]
+
+
+def test_oracle_channel_and_dm_expectation_vs_dense():
+    """The oracle's restatements of apply_qmaps.jl (supermatrix as a gate on
+    (pos, pos + n)) and expecs_dm.jl (tr(M_key rho_key) per key) against
+    dense NumPy: rho -> sum_i K_i rho K_i^dagger and tr(H rho)."""
+    import vqcb200 as V
+    from oracle import dense_np as D
+    rng = np.random.default_rng(51)
+    n = 4
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    rho = O.density_matrix(psi / np.linalg.norm(psi))
+    N = 1 << n
+    for pos, kraus in [((1,), V.Depolarizing(2, 0.2).kraus), ((3, 0), _kraus2_cpu(rng))]:
+        R = rho.reshape(N, N, order="F")
+        want = sum(D.full_operator(n, pos, K) @ R @ D.full_operator(n, pos, K).conj().T for K in kraus)
+        got = O.dm_apply_channel(rho.copy(), n, pos, kraus)
+        assert np.abs(got - want.reshape(-1, order="F")).max() < 1e-13
+        rho = got
+    terms = [O.make_term({0: "X", 2: "Y"}, 0.3), O.make_term({1: "Z"}, -1.1), O.make_term({3: "X", 0: "Z"}, 0.7j),
+             O.make_term({}, 0.25)]
+    H = D.pauli_sum_matrix(n, terms)
+    want = complex(np.trace(H @ rho.reshape(N, N, order="F")))
+    assert abs(O.dm_expectation(terms, rho, n) - want) < 1e-13

@@ -117,11 +117,98 @@ __global__ void __launch_bounds__(kRedThreads) k_dm_trace(const cplx<R>* __restr
   grid_reduce<2>(acc, s, s.result);
 }
 
+// The superoperator of a channel rho -> sum_i K_i rho K_i^dagger on k qubits
+// (apply_qmaps.jl:67-77): the 2k-qubit gate on the vectorised rho over the
+// positions (pos..., pos + n), index J = r + 2^k c (r: row bits, c: column
+// bits), S[(r, c), (r', c')] = sum_i K_i[r][r'] conj(K_i[c][c']).  mode 1:
+// S^dagger (apply_dagger!), mode 2: S^-1 (apply_inverse!).
+static int channel_supermatrix(int k, int nkraus, const double* kraus, int mode, std::vector<cd>& S) {
+  const int d = 1 << k, D = d * d;
+  S.assign((size_t)D * D, cd(0));
+  for (int i = 0; i < nkraus; ++i) {
+    const double* K = kraus + (size_t)i * d * d * 2;
+    auto at = [&](int r, int c) { return cd(K[(r * d + c) * 2], K[(r * d + c) * 2 + 1]); };
+    for (int r = 0; r < d; ++r)
+      for (int c = 0; c < d; ++c)
+        for (int r2 = 0; r2 < d; ++r2)
+          for (int c2 = 0; c2 < d; ++c2) S[(size_t)(r + d * c) * D + (r2 + d * c2)] += at(r, r2) * std::conj(at(c, c2));
+  }
+  if (mode == 1) {
+    std::vector<cd> T(S.size());
+    for (int a = 0; a < D; ++a)
+      for (int b = 0; b < D; ++b) T[(size_t)a * D + b] = std::conj(S[(size_t)b * D + a]);
+    S.swap(T);
+  } else if (mode == 2) {  // Gauss-Jordan with partial pivoting, FP64
+    std::vector<cd> A = S, I((size_t)D * D, cd(0));
+    for (int a = 0; a < D; ++a) I[(size_t)a * D + a] = 1;
+    double scale = 0;
+    for (const cd& x : A) scale = std::max(scale, std::abs(x));
+    for (int col = 0; col < D; ++col) {
+      int piv = col;
+      for (int r = col + 1; r < D; ++r)
+        if (std::abs(A[(size_t)r * D + col]) > std::abs(A[(size_t)piv * D + col])) piv = r;
+      if (std::abs(A[(size_t)piv * D + col]) <= 1e-13 * std::max(scale, 1e-300))
+        return fail(VQC_ERR_ARG, "apply_inverse!: the channel's supermatrix is singular");
+      if (piv != col)
+        for (int c = 0; c < D; ++c) {
+          std::swap(A[(size_t)piv * D + c], A[(size_t)col * D + c]);
+          std::swap(I[(size_t)piv * D + c], I[(size_t)col * D + c]);
+        }
+      const cd inv = cd(1) / A[(size_t)col * D + col];
+      for (int c = 0; c < D; ++c) {
+        A[(size_t)col * D + c] *= inv;
+        I[(size_t)col * D + c] *= inv;
+      }
+      for (int r = 0; r < D; ++r) {
+        if (r == col) continue;
+        const cd f = A[(size_t)r * D + col];
+        if (f == cd(0)) continue;
+        for (int c = 0; c < D; ++c) {
+          A[(size_t)r * D + c] -= f * A[(size_t)col * D + c];
+          I[(size_t)r * D + c] -= f * I[(size_t)col * D + c];
+        }
+      }
+    }
+    S.swap(I);
+  }
+  return VQC_OK;
+}
+
 }  // namespace vqc
 
 using namespace vqc;
 
 extern "C" {
+
+int vqc_dm_apply_channel(vqc_state rho, int k, const int* pos, int nkraus, const double* kraus, int mode) {
+  int rc = enter(rho);
+  if (rc) return rc;
+  if (!rho->n_dm) return fail(VQC_ERR_ARG, "not a density matrix");
+  if (k < 1 || k > 2)
+    return fail(VQC_ERR_UNSUPPORTED, "channels on 1 or 2 qubits (the supermatrix is a gate on 2k <= 5 qubits)");
+  if (!pos || !kraus || nkraus < 1) return fail(VQC_ERR_ARG, "channel: null positions or no Kraus operators");
+  if (mode < 0 || mode > 2) return fail(VQC_ERR_ARG, "channel: mode must be 0 (apply), 1 (dagger) or 2 (inverse)");
+  for (int i = 0; i < k; ++i) {
+    if (pos[i] < 0 || pos[i] >= rho->n_dm) return fail(VQC_ERR_ARG, "channel position out of range");
+    for (int j = 0; j < i; ++j)
+      if (pos[i] == pos[j]) return fail(VQC_ERR_ARG, "duplicate channel positions");
+  }
+  std::vector<cd> S;
+  if ((rc = channel_supermatrix(k, nkraus, kraus, mode, S))) return rc;
+  std::vector<double> m(S.size() * 2);
+  for (size_t i = 0; i < S.size(); ++i) {
+    m[2 * i] = S[i].real();
+    m[2 * i + 1] = S[i].imag();
+  }
+  int all[4];
+  for (int i = 0; i < k; ++i) {
+    all[i] = pos[i];
+    all[k + i] = pos[i] + rho->n_dm;
+  }
+  std::lock_guard<std::mutex> lk(rho->mu);
+  return apply_gate_raw(rho, 2 * k, all, m.data());
+}
+
 
 int vqc_dm_from_state(vqc_state rho, vqc_state psi) {
   int rc = enter(rho);

@@ -10,7 +10,8 @@ from .ad import back_propagate, energy_and_gradient
 from .circuit import QCircuit
 from .gates import *  # noqa: F401,F403
 from .operators import QubitsOperator, QubitsTerm, pauli
-from .state import (DensityMatrix, StateVector, apply, apply_operator, expectation, fidelity, partial_tr,
+from .state import (DensityMatrix, StateVector, apply, apply_dagger, apply_inverse, apply_operator, expectation,
+                    fidelity, partial_tr,
                     probabilities, rand_state)
 
 

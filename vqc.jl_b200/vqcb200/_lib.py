@@ -86,6 +86,8 @@ SIGNATURES = {
     "vqc_dm_ptrace": ([_H, _I, _IP, _D], _I),
     "vqc_dm_probs": ([_H, _D], _I),
     "vqc_dm_trace": ([_H, _D], _I),
+    "vqc_dm_apply_channel": ([_H, _I, _IP, _I, _D, _I], _I),
+    "vqc_dm_expect_pauli": ([_H, ctypes.POINTER(Pauli_t), _I, _D], _I),
     "vqc_expect_pauli_noalloc": ([_V, _I, _I, ctypes.POINTER(Pauli_t), _I, _V, _D], _I),
     "vqc_serve_open": ([_I, _I, _S, _I, _I, ctypes.POINTER(_H)], _I),
     "vqc_serve_submit": ([_H, _I, ctypes.POINTER(Gate_t), _I, _D, ctypes.POINTER(Param_t), _I,

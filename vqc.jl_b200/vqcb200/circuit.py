@@ -9,7 +9,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .gates import Gate
+from .gates import Gate, QuantumMap
 
 
 class QCircuit:
@@ -19,8 +19,8 @@ class QCircuit:
             self.push(g)
 
     def push(self, g):
-        if not isinstance(g, Gate):
-            raise TypeError("QCircuit holds Gate objects")
+        if not isinstance(g, (Gate, QuantumMap)):
+            raise TypeError("QCircuit holds Gate and QuantumMap objects")
         self.gates.append(g)
         self._packed = None
         return self
@@ -99,6 +99,8 @@ class Packed:
         pass
 
     def _build(self, gates, with_params):
+        if any(isinstance(g, QuantumMap) for g in gates):
+            raise TypeError("a circuit with quantum channels applies to a DensityMatrix, gate run by gate run")
         ng = len(gates)
         pks = [_gate_pack(g) for g in gates]
         chunks, offs, params = [], [], []

@@ -229,3 +229,63 @@ def CCPHASEGate(a, b, c, phi, isparas=False):
     dd = np.zeros(8, dtype=complex)
     dd[7] = 1j * e
     return Gate((a, b, c), np.diag(d), (phi,), isparas, [np.diag(dd)], name="CCPHASE")
+
+
+class QuantumMap:
+    """A quantum channel rho -> sum_i K_i rho K_i^dagger on 1 or 2 qubits
+    (QuantumCircuits.jl's QuantumMap, applied by applygates/apply_qmaps.jl).
+    Kraus matrices follow the gate conventions: bit b of an index belongs to
+    positions[b] (1-based positions)."""
+
+    def __init__(self, positions, kraus, name="QuantumMap"):
+        if isinstance(positions, int):
+            positions = (positions,)
+        self.positions = tuple(int(p) for p in positions)
+        k = len(self.positions)
+        if len(set(self.positions)) != k:
+            raise ValueError("duplicate channel positions")
+        self.kraus = [np.ascontiguousarray(np.asarray(m, dtype=np.complex128)) for m in kraus]
+        if not self.kraus or any(m.shape != (1 << k, 1 << k) for m in self.kraus):
+            raise ValueError("wrong Kraus matrix size.")
+        self.name = name
+
+    @property
+    def nqubits(self):
+        return len(self.positions)
+
+    def nparameters(self):
+        return 0
+
+    def active_parameters(self):
+        return []
+
+    def derivatives(self):
+        return []
+
+    def supermat(self):
+        """The 4^k x 4^k matrix acting on (positions, positions + n) of the
+        vectorised rho: sum_i kron(conj(K_i), K_i) (column bits high)."""
+        return sum(np.kron(m.conj(), m) for m in self.kraus)
+
+    def __repr__(self):
+        return "%s%s" % (self.name, self.positions)
+
+
+# Channel conventions (QuantumCircuits.jl is not vendored; these are the
+# standard Kraus forms, fixed here):
+#   Depolarizing(p):     sqrt(1-p) I, sqrt(p/3) X, sqrt(p/3) Y, sqrt(p/3) Z
+#   AmplitudeDamping(g): [[1, 0], [0, sqrt(1-g)]], [[0, sqrt(g)], [0, 0]]
+#   PhaseDamping(g):     [[1, 0], [0, sqrt(1-g)]], [[0, 0], [0, sqrt(g)]]
+def Depolarizing(q, p):
+    a, b = math.sqrt(1 - p), math.sqrt(p / 3)
+    return QuantumMap((q,), [a * _I, b * _X, b * _Y, b * _Z], name="Depolarizing")
+
+
+def AmplitudeDamping(q, gamma):
+    return QuantumMap((q,), [np.array([[1, 0], [0, math.sqrt(1 - gamma)]]), np.array([[0, math.sqrt(gamma)], [0, 0]])],
+                      name="AmplitudeDamping")
+
+
+def PhaseDamping(q, gamma):
+    return QuantumMap((q,), [np.array([[1, 0], [0, math.sqrt(1 - gamma)]]), np.array([[0, 0], [0, math.sqrt(gamma)]])],
+                      name="PhaseDamping")

@@ -11,7 +11,7 @@ import numpy as np
 
 from . import _lib
 from .circuit import Packed, QCircuit
-from .gates import Gate
+from .gates import Gate, QuantumMap
 from .operators import QubitsOperator, QubitsTerm
 
 _DTYPES = {np.dtype(np.complex64): _lib.VQC_C64, np.dtype(np.complex128): _lib.VQC_C128}
@@ -205,7 +205,24 @@ def apply(x, state, fuse=True):
         f = lib.vqc_dm_apply_gate if dm else lib.vqc_apply_gate
         _lib.check(f(state.handle, x.nqubits, _pos_array(x.positions), mp))
         return state
+    if isinstance(x, QuantumMap):
+        return _apply_channel(x, state, 0)
     if isinstance(x, QCircuit):
+        if any(isinstance(g, QuantumMap) for g in x):
+            # gate runs through the tile engine, channels one by one (on rho)
+            if not dm:
+                state = DensityMatrix(state)
+            run = []
+            for g in list(x) + [None]:
+                if isinstance(g, Gate):
+                    run.append(g)
+                    continue
+                if run:
+                    apply(QCircuit(run), state, fuse=fuse)
+                    run = []
+                if g is not None:
+                    _apply_channel(g, state, 0)
+            return state
         for g in x:
             if g.nqubits > 5:
                 raise NotImplementedError("only implement 5-qubit gates and less currently.")
@@ -214,6 +231,32 @@ def apply(x, state, fuse=True):
         _lib.check(f(state.handle, p.gates, p.ngates, p.mats_ptr(), 1 if fuse else 0))
         return state
     raise TypeError("apply takes a Gate or a QCircuit")
+
+
+def _apply_channel(x, state, mode):
+    """apply!(::QuantumMap, rho) (apply_qmaps.jl:5-14); a StateVector becomes
+    DensityMatrix(state) first (apply_qmaps.jl:16).  mode 1: apply_dagger!,
+    2: apply_inverse!."""
+    if not isinstance(state, DensityMatrix):
+        state = DensityMatrix(state)
+    if max(x.positions) > state.nqubits or min(x.positions) < 1:
+        raise ValueError("channel position out of range")
+    kr = np.ascontiguousarray(np.stack(x.kraus), dtype=np.complex128).view(np.float64).ravel()
+    _lib.check(_lib.load().vqc_dm_apply_channel(state.handle, x.nqubits, _pos_array(x.positions), len(x.kraus),
+                                                kr.ctypes.data_as(_lib._D), mode))
+    return state
+
+
+def apply_dagger(x, rho):
+    """apply_dagger!(::QuantumMap, rho) (apply_qmaps.jl:21-30): the adjoint of
+    the channel's supermatrix, in place."""
+    return _apply_channel(x, rho, 1)
+
+
+def apply_inverse(x, rho):
+    """apply_inverse!(::QuantumMap, rho) (apply_qmaps.jl:36-45): the inverse of
+    the channel's supermatrix, in place (raises if it is singular)."""
+    return _apply_channel(x, rho, 2)
 
 
 def _as_operator(m):
@@ -237,6 +280,13 @@ def expectation(*args):
         raise TypeError("expectation(H, psi) or expectation(phi, H, psi)")
     out = (ctypes.c_double * 2)()
     m = _as_operator(m)
+    if isinstance(psi, DensityMatrix):
+        # tr(H rho) (expecs_dm.jl:19-30)
+        if phi is not None or not isinstance(m, QubitsOperator):
+            raise TypeError("expectation(H, rho) takes a QubitsOperator / QubitsTerm")
+        arr, nt = m.packed()
+        _lib.check(lib.vqc_dm_expect_pauli(psi.handle, arr, nt, out))
+        return complex(out[0], out[1])
     if isinstance(m, QubitsOperator):
         arr, nt = m.packed()
         if phi is None:
