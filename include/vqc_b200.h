@@ -184,6 +184,13 @@ int vqc_dm_trace(vqc_state rho, double* out);
  * 1 = the supermatrix's adjoint, 2 = its inverse.  k = 1 or 2 (the
  * supermatrix is a 2k-qubit gate; the reference's gate kernels stop at 5). */
 int vqc_dm_apply_channel(vqc_state rho, int k, const int* pos, int nkraus, const double* kraus, int mode);
+/* expectation(x::DensityMatrix, m::Gate, y::DensityMatrix) of the density-
+ * matrix pullback (circuitdiff.jl:35-40): out = tr(op(a) M op(b)), FP64
+ * (re, im), with M the k-qubit matrix (row-major, index bit b <-> pos[b])
+ * acting on the row qubits (left multiplication) and op(x) = x, or x^dagger
+ * when dag_x != 0.  The reference's form is dag_a = dag_b = 0. */
+int vqc_dm_trace_prod(vqc_state a, int dag_a, vqc_state b, int dag_b, int k, const int* pos, const double* mat,
+                      double* out);
 /* expectation(::QubitsOperator, ::DensityMatrix) = tr(H rho)
  * (hamiltonian/expecs_dm/expecs_dm.jl:19-30), FP64 (re, im). */
 int vqc_dm_expect_pauli(vqc_state rho, const vqc_pauli* terms, int nterms, double* out);

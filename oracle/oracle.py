@@ -337,3 +337,40 @@ def dm_expectation(terms, rho, n):
         d = 1 << len(pos)
         r += complex(np.trace(M @ red.reshape(d, d, order="F")))
     return r
+
+
+def dm_trace_prod(a, b, n, pos, M, dag_a=False, dag_b=False):
+    """tr(op(a) M op(b)) with M on the row qubits pos (circuitdiff.jl:35-40)."""
+    N = 1 << n
+    A = a.reshape(N, N, order="F")
+    B = b.reshape(N, N, order="F")
+    A = A.conj().T if dag_a else A
+    B = B.conj().T if dag_b else B
+    MB = apply_gate(np.array(B.reshape(-1, order="F"), dtype=np.complex128), list(pos),
+                    np.asarray(M, dtype=np.complex128))
+    return complex(np.sum(A * MB.reshape(N, N, order="F").T))
+
+
+def dm_circuit_gradient(items, rho_out, delta_out, n):
+    """back_propagate for density matrices (circuitdiff.jl:42-59, 61-75).
+    items: ("gate", pos, U, [dU...]) or ("map", pos, [K...]); returns
+    (grads, delta_in, rho_in)."""
+    y, d = rho_out.copy(), delta_out.copy()
+    per = []
+    for it in reversed(items):
+        if it[0] == "map":
+            _, pos, kraus = it
+            d = dm_apply_channel(d, n, pos, kraus, mode=1)
+            y = dm_apply_channel(y, n, pos, kraus, mode=2)
+            continue
+        _, pos, U, ders = it
+        Ud = np.asarray(U, dtype=np.complex128).conj().T
+        dm_apply_gate(d, n, pos, Ud)
+        dm_apply_gate(y, n, pos, Ud)
+        g = []
+        for dU in ders:
+            D = Ud @ np.asarray(dU, dtype=np.complex128)
+            g.append((dm_trace_prod(d, y, n, pos, D, dag_a=True) + dm_trace_prod(y, d, n, pos, D.conj().T, dag_b=True)).real)
+        if g:
+            per.append(g)
+    return np.array([x for g in reversed(per) for x in g]), d, y

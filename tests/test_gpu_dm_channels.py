@@ -104,3 +104,51 @@ def test_dm_pauli_expectation(dtype, n):
     pure = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
     sv = V.expectation(H, V.StateVector(psi.astype(dtype), dtype=dtype))
     assert abs(V.expectation(H, pure) - sv) < tol(dtype) * 10 * max(1.0, abs(sv))
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("loss", ["sum", "expectation"])
+def test_noisy_dm_gradient(dtype, loss):
+    """back_propagate for density matrices with channels (circuitdiff.jl:42-59)
+    on the device against the oracle's restatement (which matches central
+    differences, test_oracle.py), for the reference's two losses
+    (check_noisy_grad.jl: real(sum(rho)) and real(expectation(H, rho)))."""
+    rng = np.random.default_rng(81)
+    n = 5
+    gates = []
+    for q in range(1, n + 1):
+        gates.append(V.U3Gate(q, *rng.uniform(0, 6, 3), isparas=True))
+    for q in range(1, n):
+        gates.append(V.CRxGate(q, q + 1, float(rng.uniform(0, 6)), isparas=True))
+    maps = [V.Depolarizing(q, 0.1) for q in range(1, n + 1)] + [V.QuantumMap((2, 4), _kraus2(rng))]
+    items = gates[:n] + maps[:3] + gates[n:] + maps[3:] + [V.RzGate(3, 0.4, isparas=True)]
+    c = V.QCircuit(items)
+    N = 1 << n
+    rho = V.apply(c, V.DensityMatrix(n, dtype=dtype))
+    terms = [({1: "X", n: "Y"}, 0.36), ({2: "Z"}, 0.7), ({1: "Z", 3: "X"}, -0.5)]
+    if loss == "sum":
+        dmat = np.ones((N, N), dtype=complex)
+    else:
+        H = D.pauli_sum_matrix(n, [O.make_term({q - 1: o for q, o in ops.items()}, cf) for ops, cf in terms])
+        dmat = H.conj().T
+    delta = V.DensityMatrix(dmat.astype(dtype), dtype=dtype)
+    ref_items = []
+    for it in items:
+        pos = [p - 1 for p in it.positions]
+        if isinstance(it, V.QuantumMap):
+            ref_items.append(("map", pos, it.kraus))
+        else:
+            ref_items.append(("gate", pos, it.mat, it.derivatives()))
+    rho_ref = O.zero_state(2 * n)
+    for it in ref_items:
+        if it[0] == "map":
+            rho_ref = O.dm_apply_channel(rho_ref, n, it[1], it[2])
+        else:
+            O.dm_apply_gate(rho_ref, n, it[1], it[2])
+    assert max_abs(rho.data(), rho_ref) < tol(dtype) * 10
+    g_ref, d_ref, y_ref = O.dm_circuit_gradient(ref_items, rho_ref, dmat.reshape(-1, order="F").copy(), n)
+    d, g, y = V.back_propagate(delta, c, rho)
+    scale = max(1.0, np.abs(g_ref).max())
+    assert np.abs(g - g_ref).max() < (1e-10 if dtype == np.complex128 else 5e-5) * scale
+    assert max_abs(y.data(), y_ref) < tol(dtype) * 100
+    assert max_abs(d.data(), d_ref) < tol(dtype) * 100 * max(1.0, np.abs(d_ref).max())

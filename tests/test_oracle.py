@@ -198,3 +198,65 @@ def test_oracle_channel_and_dm_expectation_vs_dense():
     H = D.pauli_sum_matrix(n, terms)
     want = complex(np.trace(H @ rho.reshape(N, N, order="F")))
     assert abs(O.dm_expectation(terms, rho, n) - want) < 1e-13
+
+
+def _noisy_items(n, th, p=0.1):
+    """The reference's noisy_circuit (test/check_noisy_grad.jl:3-9): a
+    variational circuit (RY on every qubit, CRX chain, RZ) and a layer of
+    Depolarizing channels, as oracle items (0-based positions)."""
+    import vqcb200 as V
+    items, k = [], 0
+    for q in range(n):
+        g = V.RyGate(q + 1, th[k], isparas=True)
+        items.append(("gate", [q], g.mat, g.derivatives()))
+        k += 1
+    for q in range(n - 1):
+        g = V.CRxGate(q + 1, q + 2, th[k], isparas=True)
+        items.append(("gate", [q, q + 1], g.mat, g.derivatives()))
+        k += 1
+    for q in range(n):
+        g = V.RzGate(q + 1, th[k], isparas=True)
+        items.append(("gate", [q], g.mat, g.derivatives()))
+        k += 1
+    for q in range(n):
+        items.append(("map", [q], V.Depolarizing(q + 1, p).kraus))
+    return items
+
+
+def _dm_forward(items, rho, n):
+    rho = rho.copy()
+    for it in items:
+        if it[0] == "map":
+            rho = O.dm_apply_channel(rho, n, it[1], it[2])
+        else:
+            O.dm_apply_gate(rho, n, it[1], it[2])
+    return rho
+
+
+@pytest.mark.parametrize("loss", ["sum", "expectation"])
+def test_oracle_noisy_dm_gradient_vs_fd(loss):
+    """circuitdiff.jl:42-59 restated (gates: uncompute + Re[tr(D^+ D y) +
+    tr(y D^+ D^+)], channels: S^+ on the cotangent, S^-1 on the state)
+    against 5-point-free central differences, h = 1e-4 (check_noisy_grad.jl)."""
+    from oracle import dense_np as D
+    n = 3
+    rng = np.random.default_rng(71)
+    th = rng.uniform(0, 2 * np.pi, 3 * n - 1)
+    N = 1 << n
+    rho0 = O.zero_state(2 * n)  # DensityMatrix(n) = |0><0|
+    terms = [O.make_term({0: "X", 2: "Y"}, 0.36), O.make_term({1: "Z"}, 0.7), O.make_term({0: "Z", 1: "X"}, -0.5)]
+    H = D.pauli_sum_matrix(n, terms)
+
+    def L(t):
+        r = _dm_forward(_noisy_items(n, t), rho0, n)
+        if loss == "sum":
+            return np.sum(r).real
+        return np.trace(H @ r.reshape(N, N, order="F")).real
+
+    out = _dm_forward(_noisy_items(n, th), rho0, n)
+    delta = np.ones(N * N, dtype=complex) if loss == "sum" else H.conj().T.reshape(-1, order="F").copy()
+    g, _, rho_in = O.dm_circuit_gradient(_noisy_items(n, th), out, delta, n)
+    h = 1e-4
+    fd = np.array([(L(th + h * e) - L(th - h * e)) / (2 * h) for e in np.eye(th.size)])
+    assert np.abs(g - fd).max() < 1e-6
+    assert np.abs(rho_in - rho0).max() < 1e-10

@@ -10,6 +10,7 @@
 // positions (pos, pos + n) in ONE pass (half the HBM traffic), and in two
 // passes for k >= 3 (W would exceed the 5-qubit kernel limit).
 #include <algorithm>
+#include <mutex>
 
 #include "engine.h"
 #include "subspace.cuh"
@@ -117,6 +118,78 @@ __global__ void __launch_bounds__(kRedThreads) k_dm_trace(const cplx<R>* __restr
   grid_reduce<2>(acc, s, s.result);
 }
 
+// tr(op(A) M op(B)) for two density matrices (circuitdiff.jl:35-40, the
+// expectation(x::DensityMatrix, m::Gate, y::DensityMatrix) of the DM
+// pullback): M is a K-qubit operator on the row index (left
+// multiplication), op = identity or the conjugate transpose.  Work item =
+// (column j, row group r0 with the K target bits clear):
+//   (M B)[r_s][j] = sum_t M[s][t] B[r_t][j],  sum_s A[j][r_s] (M B)[r_s][j].
+// FP64 accumulation and grid reduction.
+template <int K>
+struct TraceProdArgs {
+  double2 M[(1 << K) * (1 << K)];  // sorted-position order, row-major
+  int64_t off[1 << K];             // row offset of target pattern t
+  int sp[K];                       // sorted target bits
+};
+
+template <class R, int K>
+__global__ void __launch_bounds__(kRedThreads)
+    k_dm_trace_prod(const cplx<R>* __restrict__ a, const cplx<R>* __restrict__ b, int n, int dag_a, int dag_b,
+                    const __grid_constant__ TraceProdArgs<K> g, Scratch s, double* res) {
+  constexpr int D = 1 << K;
+  const int64_t N = int64_t(1) << n, rows = N >> K, items = rows << n;
+  double acc[2] = {0, 0};
+  for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = it >> (n - K);
+    int64_t r0 = it & (rows - 1);
+#pragma unroll
+    for (int q = 0; q < K; ++q) r0 = ((r0 >> g.sp[q]) << (g.sp[q] + 1)) | (r0 & ((int64_t(1) << g.sp[q]) - 1));
+    double2 bv[D];
+#pragma unroll
+    for (int t = 0; t < D; ++t) {
+      const int64_t r = r0 + g.off[t];
+      bv[t] = dag_b ? to_d2(b[j + N * r]) : to_d2(b[r + N * j]);
+      if (dag_b) bv[t].y = -bv[t].y;
+    }
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      double2 mb = make_double2(0, 0);
+#pragma unroll
+      for (int t = 0; t < D; ++t) mb = cfma(g.M[q * D + t], bv[t], mb);
+      const int64_t r = r0 + g.off[q];
+      double2 av = dag_a ? to_d2(a[r + N * j]) : to_d2(a[j + N * r]);
+      if (dag_a) av.y = -av.y;
+      acc[0] = fma(av.x, mb.x, fma(-av.y, mb.y, acc[0]));
+      acc[1] = fma(av.x, mb.y, fma(av.y, mb.x, acc[1]));
+    }
+  }
+  grid_reduce<2>(acc, s, res);
+}
+
+template <int K>
+static int trace_prod_k(vqc_state a, vqc_state b, int dag_a, int dag_b, const int* sp, const std::vector<cd>& M,
+                        double* out) {
+  TraceProdArgs<K> g;
+  for (int i = 0; i < (1 << K) * (1 << K); ++i) g.M[i] = make_double2(M[i].real(), M[i].imag());
+  for (int q = 0; q < K; ++q) g.sp[q] = sp[q];
+  for (int t = 0; t < (1 << K); ++t) g.off[t] = offset_of(t, K, sp);
+  const int n = b->n_dm;
+  const int grid = reduction_grid(b->device, (int64_t(1) << (2 * n - K)));
+  ProfScope prof(b->stream, "dm_trace_prod", 2.0 * (double)b->size() * b->amp_bytes());
+  if (b->dtype == VQC_C64)
+    k_dm_trace_prod<float, K><<<grid, kRedThreads, 0, b->stream>>>((const float2*)a->d, (const float2*)b->d, n, dag_a,
+                                                                    dag_b, g, b->scr, b->scr.result);
+  else
+    k_dm_trace_prod<double, K><<<grid, kRedThreads, 0, b->stream>>>((const double2*)a->d, (const double2*)b->d, n,
+                                                                     dag_a, dag_b, g, b->scr, b->scr.result);
+  VQC_CK(cudaGetLastError());
+  int rc = fetch_result(b, 2);
+  if (rc) return rc;
+  out[0] = b->h_result[0];
+  out[1] = b->h_result[1];
+  return VQC_OK;
+}
+
 // The superoperator of a channel rho -> sum_i K_i rho K_i^dagger on k qubits
 // (apply_qmaps.jl:67-77): the 2k-qubit gate on the vectorised rho over the
 // positions (pos..., pos + n), index J = r + 2^k c (r: row bits, c: column
@@ -179,6 +252,33 @@ static int channel_supermatrix(int k, int nkraus, const double* kraus, int mode,
 using namespace vqc;
 
 extern "C" {
+
+int vqc_dm_trace_prod(vqc_state a, int dag_a, vqc_state b, int dag_b, int k, const int* pos, const double* mat,
+                      double* out) {
+  int rc = enter(b);
+  if (rc) return rc;
+  if (!a || !a->n_dm || !b->n_dm || a->n_dm != b->n_dm || a->dtype != b->dtype || a->device != b->device)
+    return fail(VQC_ERR_ARG, "tr(A M B): two density matrices of the same size, dtype and device");
+  if (!out || !pos || !mat) return fail(VQC_ERR_ARG, "null argument");
+  if (k < 1 || k > 5) return fail(VQC_ERR_UNSUPPORTED, "only implement 5-qubit gates and less currently.");
+  if (k > b->n_dm) return fail(VQC_ERR_ARG, "operator wider than the register");
+  int sp[5];
+  std::vector<cd> M;
+  if ((rc = order_matrix(b->n_dm, k, pos, mat, sp, M))) return rc;
+  std::lock_guard<std::mutex> lk(b->mu);
+  std::unique_lock<std::mutex> la(a->mu, std::defer_lock);
+  if (a != b) la.lock();
+  if (a != b && (rc = stream_after(b, a))) return rc;
+  switch (k) {
+    case 1: rc = trace_prod_k<1>(a, b, dag_a, dag_b, sp, M, out); break;
+    case 2: rc = trace_prod_k<2>(a, b, dag_a, dag_b, sp, M, out); break;
+    case 3: rc = trace_prod_k<3>(a, b, dag_a, dag_b, sp, M, out); break;
+    case 4: rc = trace_prod_k<4>(a, b, dag_a, dag_b, sp, M, out); break;
+    default: rc = trace_prod_k<5>(a, b, dag_a, dag_b, sp, M, out); break;
+  }
+  if (rc) return rc;
+  return a != b ? stream_after(a, b) : VQC_OK;
+}
 
 int vqc_dm_apply_channel(vqc_state rho, int k, const int* pos, int nkraus, const double* kraus, int mode) {
   int rc = enter(rho);
