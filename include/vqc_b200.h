@@ -96,6 +96,11 @@ int vqc_state_download(vqc_state h, void* host, size_t bytes);
 int vqc_state_reset(vqc_state h);
 /* copy(x) (statevector.jl:30): same qubit count; converts FP32 <-> FP64. */
 int vqc_state_copy(vqc_state dst, vqc_state src);
+/* The state with qubit q (0-based) fixed at `value` and removed, times
+ * `scale`: dst (one qubit fewer) <- scale * <value|_q src.  The collapsed
+ * state of measure(psi, q) (measure.jl:38-46) and post_select(psi, q, v)
+ * without keep (postselect.jl:37-44), scale = 1/sqrt(probability). */
+int vqc_state_take_qubit(vqc_state src, int q, int value, double scale, vqc_state dst);
 /* norm(x) (statevector.jl:53), FP64. */
 int vqc_state_norm(vqc_state h, double* out);
 /* dot(x, y) = <x|y> (statevector.jl:54), FP64; out = (re, im). */

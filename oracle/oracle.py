@@ -374,3 +374,26 @@ def dm_circuit_gradient(items, rho_out, delta_out, n):
         if g:
             per.append(g)
     return np.array([x for g in reversed(per) for x in g]), d, y
+
+
+# ----------------------------------------------------------------------------- measurement
+def sv_prob_zero(v, q):
+    """compute_probability_zero(v, key) (measure.jl:47-59): sum of |v_i|^2
+    over the indices with bit q clear (0-based q)."""
+    idx = np.arange(v.size)
+    return float(np.sum(np.abs(v[(idx >> q) & 1 == 0]) ** 2))
+
+
+def collapse(v, q, i, p, reset):
+    """The collapse of apply!(::QMeasure, ...) (measure.jl:4-16) on a state
+    vector: |i> -> |0> (reset) or |i>, scaled by 1/sqrt(p), other branch 0."""
+    m = np.zeros((2, 2), dtype=complex)
+    m[0 if reset else i, i] = 1 / np.sqrt(p)
+    return apply_gate(np.array(v, dtype=np.complex128), [q], m)
+
+
+def take_qubit(v, q, value):
+    """The slice of qubit q at `value` (measure.jl:38-46, postselect.jl:37-44:
+    swap the qubit to position 1, keep one row of the 2 x L/2 reshape)."""
+    idx = np.arange(v.size)
+    return np.array(v[(idx >> q) & 1 == value], dtype=np.complex128)

@@ -167,6 +167,19 @@ __global__ void k_set_basis(cplx<R>* v, int64_t N, int64_t one) {
     v[i] = mkc<R>(i == one ? R(1) : R(0), R(0));
 }
 
+// The slice of qubit q at `value`, scaled: dst[j] = scale * src[j with bit
+// `value` inserted at q] (measure / post_select dropping the qubit,
+// measure.jl:38-46, postselect.jl:37-44).
+template <class R>
+__global__ void k_take_qubit(cplx<R>* __restrict__ dst, const cplx<R>* __restrict__ src, int64_t M, int q, int value,
+                             double scale) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < M; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = ((j >> q) << (q + 1)) | ((int64_t)value << q) | (j & ((int64_t(1) << q) - 1));
+    const cplx<R> a = src[i];
+    dst[j] = mkc<R>((R)(scale * a.x), (R)(scale * a.y));
+  }
+}
+
 template <class RD, class RS>
 __global__ void k_convert(cplx<RD>* dst, const cplx<RS>* src, int64_t N) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
@@ -339,6 +352,25 @@ int vqc_state_reset(vqc_state h) {
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(h->mu);
   return set_basis(h, 0);
+}
+
+int vqc_state_take_qubit(vqc_state src, int q, int value, double scale, vqc_state dst) {
+  int rc = enter(src);
+  if (rc) return rc;
+  if (!dst || src->n_dm || dst->n_dm || src->nq < 1 || dst->nq != src->nq - 1 || dst->dtype != src->dtype ||
+      dst->device != src->device)
+    return fail(VQC_ERR_ARG, "take_qubit: dst must be a state of one qubit fewer, same dtype and device");
+  if (q < 0 || q >= src->nq || (value != 0 && value != 1)) return fail(VQC_ERR_ARG, "take_qubit: bad qubit or value");
+  std::lock_guard<std::mutex> lk(src->mu);
+  if ((rc = stream_after(src, dst))) return rc;
+  const int64_t M = dst->size();
+  const int g = launch_grid(src->device, M);
+  if (src->dtype == VQC_C64)
+    k_take_qubit<float><<<g, 256, 0, src->stream>>>((float2*)dst->d, (const float2*)src->d, M, q, value, scale);
+  else
+    k_take_qubit<double><<<g, 256, 0, src->stream>>>((double2*)dst->d, (const double2*)src->d, M, q, value, scale);
+  VQC_CK(cudaGetLastError());
+  return stream_after(dst, src);
 }
 
 int vqc_state_copy(vqc_state dst, vqc_state src) {
