@@ -96,6 +96,10 @@ int vqc_state_download(vqc_state h, void* host, size_t bytes);
 int vqc_state_reset(vqc_state h);
 /* copy(x) (statevector.jl:30): same qubit count; converts FP32 <-> FP64. */
 int vqc_state_copy(vqc_state dst, vqc_state src);
+/* y <- a x + b y, a and b complex (re, im): the vector update of the Krylov
+ * solvers behind ground_state / time_evolution (utility/groundstate.jl:4-25,
+ * KrylovKit's eigsolve / exponentiate with the operator's matvec). */
+int vqc_state_axpby(vqc_state y, const double* a, vqc_state x, const double* b);
 /* The state with qubit q (0-based) fixed at `value` and removed, times
  * `scale`: dst (one qubit fewer) <- scale * <value|_q src.  The collapsed
  * state of measure(psi, q) (measure.jl:38-46) and post_select(psi, q, v)

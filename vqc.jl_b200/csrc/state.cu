@@ -180,6 +180,17 @@ __global__ void k_take_qubit(cplx<R>* __restrict__ dst, const cplx<R>* __restric
   }
 }
 
+// y <- a x + b y (complex a, b), the vector update of the Krylov methods.
+template <class R>
+__global__ void k_axpby(cplx<R>* __restrict__ y, const cplx<R>* __restrict__ x, int64_t N, double2 a, double2 b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 xv = to_d2(x[i]), yv = to_d2(y[i]);
+    const double re = a.x * xv.x - a.y * xv.y + b.x * yv.x - b.y * yv.y;
+    const double im = a.x * xv.y + a.y * xv.x + b.x * yv.y + b.y * yv.x;
+    y[i] = mkc<R>((R)re, (R)im);
+  }
+}
+
 template <class RD, class RS>
 __global__ void k_convert(cplx<RD>* dst, const cplx<RS>* src, int64_t N) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
@@ -352,6 +363,25 @@ int vqc_state_reset(vqc_state h) {
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(h->mu);
   return set_basis(h, 0);
+}
+
+int vqc_state_axpby(vqc_state y, const double* a, vqc_state x, const double* b) {
+  int rc = enter(y);
+  if (rc) return rc;
+  if (!x || !a || !b || x->nq != y->nq || x->dtype != y->dtype || x->device != y->device)
+    return fail(VQC_ERR_ARG, "axpby: same size, dtype and device");
+  std::lock_guard<std::mutex> lk(y->mu);
+  std::unique_lock<std::mutex> lx(x->mu, std::defer_lock);
+  if (x != y) lx.lock();
+  if (x != y && (rc = stream_after(y, x))) return rc;
+  const int g = launch_grid(y->device, y->size());
+  const double2 da = make_double2(a[0], a[1]), db = make_double2(b[0], b[1]);
+  if (y->dtype == VQC_C64)
+    k_axpby<float><<<g, 256, 0, y->stream>>>((float2*)y->d, (const float2*)x->d, y->size(), da, db);
+  else
+    k_axpby<double><<<g, 256, 0, y->stream>>>((double2*)y->d, (const double2*)x->d, y->size(), da, db);
+  VQC_CK(cudaGetLastError());
+  return x != y ? stream_after(x, y) : VQC_OK;
 }
 
 int vqc_state_take_qubit(vqc_state src, int q, int value, double scale, vqc_state dst) {

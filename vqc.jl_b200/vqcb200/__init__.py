@@ -9,6 +9,7 @@ from . import _lib
 from .ad import back_propagate, energy_and_gradient
 from .circuit import QCircuit
 from .gates import *  # noqa: F401,F403
+from .krylov import ground_state, time_evolution
 from .measure import measure, measure_inplace, post_select, post_select_inplace, prob_zero
 from .operators import QubitsOperator, QubitsTerm, pauli
 from .state import (DensityMatrix, StateVector, apply, apply_dagger, apply_inverse, apply_operator, expectation,

@@ -88,6 +88,7 @@ SIGNATURES = {
     "vqc_dm_trace": ([_H, _D], _I),
     "vqc_dm_apply_channel": ([_H, _I, _IP, _I, _D, _I], _I),
     "vqc_state_take_qubit": ([_H, _I, _I, ctypes.c_double, _H], _I),
+    "vqc_state_axpby": ([_H, _D, _H, _D], _I),
     "vqc_dm_trace_prod": ([_H, _I, _H, _I, _I, _IP, _D, _D], _I),
     "vqc_dm_expect_pauli": ([_H, ctypes.POINTER(Pauli_t), _I, _D], _I),
     "vqc_expect_pauli_noalloc": ([_V, _I, _I, ctypes.POINTER(Pauli_t), _I, _V, _D], _I),
