@@ -9,8 +9,9 @@ thread bits and on qubits outside the tile are tested at run time.  These
 circuits put every form on qubit 0, on low, middle and high qubits, with
 controls on each kind of bit, controls on |0>, two controls, dense two-qubit
 gates and diagonal gates, at n = 14 (tile of 12 qubits, 2 qubits outside).  Each case runs
-through the interpreted kernel (VQC_JIT=off) and through the kernels compiled
-at run time for each pass structure (VQC_JIT=on).
+through the generic tile kernel (VQC_JIT=off), the kernels compiled at run
+time for each pass structure (VQC_JIT=on) and their interpreted fallback on
+the same packed plan (VQC_JIT=interp).
 Tolerances: FP32 amplitudes 1e-5 (helpers.tol) scaled by the circuit depth.
 """
 import numpy as np
@@ -22,7 +23,7 @@ from oracle import gates_ref as GR
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
-JIT = ["off", "on"]
+JIT = ["off", "on", "interp"]
 
 N = 14
 ONE_Q = [1, 2, 3, 7, 12, 14]  # 1-based: qubit 0 (lane bit), low, middle, high, outside the first tile

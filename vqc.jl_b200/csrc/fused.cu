@@ -278,14 +278,14 @@ __device__ __forceinline__ void dispatch_u2(int ra, int rb, cplx<R> (&v)[16], cp
 #define VQC_MINB_F32_FWD 3
 #endif
 #ifndef VQC_MINB_F32_ADJ
-#define VQC_MINB_F32_ADJ 1
+#define VQC_MINB_F32_ADJ 2
 #endif
-template <class R, bool ADJ>
+template <class R, bool ADJ, bool PACKED>
 struct MinBlocks {
   static constexpr int value = 2;
 };
 template <bool ADJ>
-struct MinBlocks<float, ADJ> {
+struct MinBlocks<float, ADJ, true> {
   static constexpr int value = ADJ ? VQC_MINB_F32_ADJ : VQC_MINB_F32_FWD;
 };
 
@@ -446,31 +446,34 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
   }
 }
 
-// One pass of one state (the single-request path).  FP32 states run the
-// packed body (tile_f32.cuh), FP64 states the body above.
-template <class R, int M, bool ADJ, bool GEN>
+// One pass of one state.  PACKED: the FP32 packed body (tile_f32.cuh) on a
+// plan laid out for it (lane bit in every stage, DevStageF); it is the
+// interpreted form of the run-time compiled passes and runs only where a
+// compiled kernel is missing.  Otherwise the body above (FP64, and FP32
+// passes that are interpreted: the serving loop, small states).
+template <class R, int M, bool ADJ, bool GEN, bool PACKED>
 __device__ __forceinline__ void tile_run(cplx<R>* psi, cplx<R>* lam, const DevPass* pass, const void* stages,
                                          const DevOp* ops, const cplx<R>* pool, double* partials, int ncta) {
-  if constexpr (std::is_same<R, float>::value)
+  if constexpr (PACKED && std::is_same<R, float>::value)
     f32t::tile_body<M, ADJ, GEN>(psi, lam, pass, (const DevStageF*)stages, ops, pool, partials, ncta);
   else
     tile_body<R, M, ADJ, GEN>(psi, lam, pass, (const DevStage*)stages, ops, pool, partials, ncta);
 }
 
-template <class R, int M, bool ADJ, bool GEN>
-__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
+template <class R, int M, bool ADJ, bool GEN, bool PACKED>
+__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ, PACKED>::value)
     k_tile(cplx<R>* psi, cplx<R>* lam, const DevPass* pass, const void* stages, const DevOp* ops,
            const cplx<R>* pool, double* partials) {
-  tile_run<R, M, ADJ, GEN>(psi, lam, pass, stages, ops, pool, partials, gridDim.x);
+  tile_run<R, M, ADJ, GEN, PACKED>(psi, lam, pass, stages, ops, pool, partials, gridDim.x);
 }
 
 template <class R, int M, bool ADJ>
-__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ>::value)
+__global__ void __launch_bounds__(1 << (M - kRegBits), MinBlocks<R, ADJ, false>::value)
     k_tile_batch(const TileItem* __restrict__ items) {
   const TileItem it = items[blockIdx.y];
   if ((int)blockIdx.x >= it.ncta) return;
-  tile_run<R, M, ADJ, true>((cplx<R>*)it.psi, (cplx<R>*)it.lam, it.pass, it.stages, it.ops, (const cplx<R>*)it.pool,
-                            it.partials, it.ncta);
+  tile_run<R, M, ADJ, true, false>((cplx<R>*)it.psi, (cplx<R>*)it.lam, it.pass, it.stages, it.ops,
+                                   (const cplx<R>*)it.pool, it.partials, it.ncta);
 }
 
 // Sums the per-CTA partials over the grid in a fixed order: block = slot.
@@ -721,12 +724,12 @@ static void plan_passes(int n, const TileConfig& tc, bool adj, std::vector<PItem
 }
 
 // Conflict check of a register-bit set for the shared-memory swizzle.
-// FP64: 16-byte amplitudes, quarter-warps over the tile swizzle Swz<double>.
-// FP32 (packed): 16-byte pairs, the lowest three thread bits (tile bits
-// outside rs, ascending) must fall in distinct classes of the pair swizzle,
-// class = (tile bit - 1) mod 3.
-static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype) {
-  if (dtype == VQC_C64) {
+// FP64: 16-byte amplitudes, quarter-warps over the tile swizzle Swz<double>;
+// FP32: 8-byte amplitudes, half-warps over Swz<float>.  Packed FP32: 16-byte
+// pairs, the lowest three thread bits (tile bits outside rs, ascending) must
+// fall in distinct classes of the pair swizzle, class = (tile bit - 1) mod 3.
+static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype, bool packed) {
+  if (packed) {
     int seen = 0, k = 0;
     for (int b = 1; b < M && k < 3; ++b) {
       if (std::find(rs.begin(), rs.end(), b) != rs.end()) continue;
@@ -738,11 +741,15 @@ static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype) {
     return true;
   }
   std::vector<int> lanes;
-  for (int b = 0; b < M && (int)lanes.size() < 3; ++b)
+  for (int b = 0; b < M && (int)lanes.size() < (dtype == VQC_C64 ? 4 : 3); ++b)
     if (std::find(rs.begin(), rs.end(), b) == rs.end()) lanes.push_back(b);
   int seen = 0;
   for (int b : lanes) {
-    const int res = b < 3 ? b : (b < 9 ? (b - 3) % 3 : -1);
+    int res;
+    if (dtype == VQC_C64)
+      res = b < 4 ? b : (b < 8 ? b - 4 : -1);
+    else
+      res = b < 3 ? b : (b < 9 ? (b - 3) % 3 : -1);
     if (res < 0 || (seen >> res & 1)) return false;
     seen |= 1 << res;
   }
@@ -754,8 +761,8 @@ static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype) {
 // of the packed layout).  The free bits left over are filled preferring the
 // stage's control bits (register controls are compile-time cases in the FP32
 // body), then a bank-conflict-free layout.
-static void plan_stages(PlanPass& p, int M, int dtype) {
-  const bool lane0 = dtype == VQC_C64;
+static void plan_stages(PlanPass& p, int M, int dtype, bool packed) {
+  const bool lane0 = packed;
   std::map<int, int> tbit;  // global qubit -> tile bit
   for (int b = 0; b < (int)p.tile_q.size(); ++b) tbit[p.tile_q[b]] = b;
   std::vector<int> pending(p.ops.size());
@@ -812,7 +819,7 @@ static void plan_stages(PlanPass& p, int M, int dtype) {
         if (mask >> i & 1) t.push_back(cand[i]);
       std::sort(t.begin(), t.end());
       if (best.empty()) best = t;
-      if (rs_conflict_free(t, M, dtype)) {
+      if (rs_conflict_free(t, M, dtype, packed)) {
         best = t;
         found = true;
       }
@@ -841,14 +848,23 @@ static size_t pass_smem(const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t npool = (size_t)ps.npool * sizeof(cplx<R>);
   return tile_bytes<R, M, ADJ>() + (ADJ ? (size_t)ps.nslots * (NT / 32) * 8 * sizeof(double) : 0) +
-         (std::is_same<R, float>::value ? sizeof(DevStageF) : sizeof(DevStage)) * ps.nstages + sizeof(DevOp) * ps.nops + ((npool + 15) & ~size_t(15));
+         (ps.packed ? sizeof(DevStageF) : sizeof(DevStage)) * ps.nstages + sizeof(DevOp) * ps.nops +
+         ((npool + 15) & ~size_t(15));
+}
+
+// The tile kernel of a pass shape.
+template <class R, int M, bool ADJ>
+static auto tile_kernel(const PassShape& ps) -> decltype(&k_tile<R, M, ADJ, true, false>) {
+  if constexpr (std::is_same<R, float>::value)
+    if (ps.packed) return ps.general ? k_tile<R, M, ADJ, true, true> : k_tile<R, M, ADJ, false, true>;
+  return ps.general ? k_tile<R, M, ADJ, true, false> : k_tile<R, M, ADJ, false, false>;
 }
 
 template <class R, int M, bool ADJ>
 static int tile_grid(int device, const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t smem = pass_smem<R, M, ADJ>(ps);
-  auto kfun = ps.general ? k_tile<R, M, ADJ, true> : k_tile<R, M, ADJ, false>;
+  auto kfun = tile_kernel<R, M, ADJ>(ps);
   cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, NT, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
@@ -860,7 +876,7 @@ static int launch_tile(vqc_state h, void* psi, void* lam, const DevPass* dp, con
                        const void* pool, double* partials, int grid, const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
   const size_t smem = pass_smem<R, M, ADJ>(ps);
-  auto kfun = ps.general ? k_tile<R, M, ADJ, true> : k_tile<R, M, ADJ, false>;
+  auto kfun = tile_kernel<R, M, ADJ>(ps);
   VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
   ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward",
                  (double)(ADJ ? 4 : 2) * h->size() * sizeof(cplx<R>));
@@ -1048,7 +1064,8 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
 }
 
 template <class R, int M, bool ADJ>
-static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, SerialPlan& sp, std::vector<AccRef>* accs) {
+static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, SerialPlan& sp, std::vector<AccRef>* accs,
+                           bool packed = false) {
   Device d;
   std::vector<cplx<R>> pool;
   std::vector<PassLoc>& locs = sp.locs;
@@ -1061,7 +1078,7 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
       locs[pi].gate = p.gate;
       continue;
     }
-    plan_stages(p, M, dtype);
+    plan_stages(p, M, dtype, packed);
     std::vector<DevStage> ds;
     std::vector<DevOp> dops;
     std::map<int, int> tbit;
@@ -1074,8 +1091,10 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
     std::vector<DevStageF> dsf;
     for (const PlanStage& st : p.stages) {
       if constexpr (std::is_same<R, float>::value) {
-        stage_f32(p, st, M, n, tile_mask, tbit, ADJ, slot, row, dsf, dops, pool, pool_begin, accs);
-        continue;
+        if (packed) {
+          stage_f32(p, st, M, n, tile_mask, tbit, ADJ, slot, row, dsf, dops, pool, pool_begin, accs);
+          continue;
+        }
       }
       DevStage s{};
       uint32_t rsmask = 0;
@@ -1177,10 +1196,11 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
     P.stage_begin = 0;
     P.stage_end = (int)p.stages.size();
     locs[pi].pass = d.put(&P, 1);
-    if constexpr (std::is_same<R, float>::value)
+    if (packed)
       locs[pi].stages = d.put(dsf.data(), dsf.size());
     else
       locs[pi].stages = d.put(ds.data(), ds.size());
+    locs[pi].shape.packed = packed;
     // op indices in stages are local to this pass's op array
     locs[pi].ops = d.put(dops.data(), std::max<size_t>(dops.size(), 1));
   }
@@ -1240,20 +1260,24 @@ static bool use_jit(const vqc_state h) {
   const int mode = jit_mode();
   return h->dtype == VQC_C64 && (mode == 1 || (mode == 2 && h->nq >= 18)) && jit_available();
 }
+// The packed FP32 plan layout: for the compiled passes, or forced with
+// VQC_JIT=interp (the packed interpreter, the compiled kernels' fallback).
+static bool use_packed(const vqc_state h) { return h->dtype == VQC_C64 && (use_jit(h) || jit_mode() == 3); }
 
 template <class R, int M, bool ADJ>
 static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
                     std::vector<AccRef>* accs, double* rows_dev) {
   const int n = h->nq;
   SerialPlan sp;
-  serialize_plan<R, M, ADJ>(n, h->dtype, passes, sp, accs);
+  const bool packed = use_packed(h);
+  serialize_plan<R, M, ADJ>(n, h->dtype, passes, sp, accs, packed);
   note_plan(ADJ, passes);
   const std::vector<PassLoc>& locs = sp.locs;
   const size_t pool_off = sp.pool_off;
   // run-time specialised kernels (FP32), one per pass structure
   std::vector<const void*> jk(passes.size(), nullptr);
   if constexpr (std::is_same<R, float>::value) {
-    if (use_jit(h)) {
+    if (packed && use_jit(h)) {
       std::vector<JitPassRef> refs(passes.size());
       for (size_t pi = 0; pi < passes.size(); ++pi)
         if (!locs[pi].standalone)

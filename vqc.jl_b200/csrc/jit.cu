@@ -14,10 +14,11 @@
 // stays run-time data in the pass's descriptors, exactly as the interpreter
 // reads them.
 //
-// VQC_JIT=0 / off: never (the interpreter runs every pass); 1 / on: every
-// FP32 tile pass; auto (default): passes of states with at least 2^18
-// amplitudes.  If NVRTC cannot be loaded, or a compilation fails, the pass
-// runs on the interpreter (also a GPU kernel).
+// VQC_JIT=0 / off: never (the generic tile kernel runs every pass); 1 / on:
+// every FP32 tile pass; auto (default): passes of states with at least 2^18
+// amplitudes; interp: the packed plan on its interpreter (testing).  If
+// NVRTC cannot be loaded the generic kernel runs; if one compilation fails,
+// that pass runs on the packed interpreter (both are GPU kernels).
 #include <dlfcn.h>
 #include <nvrtc.h>
 
@@ -168,6 +169,7 @@ int jit_mode() {
   const char* v = std::getenv("VQC_JIT");
   if (!v || !*v || !std::strcmp(v, "auto")) return 2;
   if (!std::strcmp(v, "0") || !std::strcmp(v, "off")) return 0;
+  if (!std::strcmp(v, "interp")) return 3;
   return 1;
 }
 

@@ -55,6 +55,7 @@ struct FOp {
 struct PassShape {
   int nslots = 0, nstages = 0, nops = 0, npool = 0;
   bool general = true;  // false: every op of the pass is a one-qubit op
+  bool packed = false;  // FP32 packed layout (DevStageF), for the compiled pass kernels
 };
 
 // An accumulating op of the reverse sweep and the row of 8 doubles (the
@@ -137,7 +138,7 @@ struct ReqPlan {
 };
 
 // Run-time specialised FP32 tile kernels (jit.cu).
-int jit_mode();        // 0 off, 1 on, 2 auto (VQC_JIT)
+int jit_mode();        // 0 off, 1 on, 2 auto, 3 packed interpreter (VQC_JIT)
 bool jit_available();  // NVRTC could be loaded
 int jit_min_blocks(bool adj, int M);
 // Source of a pass's kernel ("" when the pass is not compiled: its matrix
