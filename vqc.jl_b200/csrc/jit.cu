@@ -176,10 +176,11 @@ int jit_mode() {
 bool jit_available() { return nvrtc().ok; }
 
 // Resident CTAs per SM the compiled kernels' registers are budgeted for:
-// 768 threads for forward passes, 512 for the reverse sweep.
+// 1024 threads for forward passes (64 registers), 512 for the reverse sweep
+// (128 registers).
 int jit_min_blocks(bool adj, int M) {
   const int nt = 1 << (M - kRegBits);
-  return adj ? env_int("VQC_JIT_MINB_ADJ", 512 / nt) : env_int("VQC_JIT_MINB_FWD", 768 / nt);
+  return adj ? env_int("VQC_JIT_MINB_ADJ", 512 / nt) : env_int("VQC_JIT_MINB_FWD", 1024 / nt);
 }
 
 std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool) {
