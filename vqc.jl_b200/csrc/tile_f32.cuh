@@ -312,11 +312,11 @@ __device__ __forceinline__ void pack_lane(const u64 (&c)[4], float (&s)[8]) {
 }
 
 // Thread partials -> the warp's slot row in shared memory.  A warp
-// reduce-scatter of the 8 values: the first two levels (lanes 16 and 8
-// apart) in FP32, so each partial then sums at most 32 products; the last
-// three levels and everything after them (warps, CTAs, the grid) in FP64.
-// Afterwards lane L with L % 4 == 0 holds the warp total of value L / 4.
-// Every lane of the warp must call it.
+// reduce-scatter of the 8 values in FP32 (each warp partial sums at most 256
+// products: 32 lanes x 8 amplitude pairs); the warp partials are added in
+// FP64 into the warp's slot row, and every later level (warps, CTAs, the
+// grid) is FP64.  Afterwards lane L with L % 4 == 0 holds the warp total of
+// value L / 4.  Every lane of the warp must call it.
 __device__ __forceinline__ void flush8(const float (&s)[8], double* sacc, int slot, int nwarps) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
@@ -331,11 +331,10 @@ __device__ __forceinline__ void flush8(const float (&s)[8], double* sacc, int sl
     const float keep = b3 ? y[i + 2] : y[i], send = b3 ? y[i] : y[i + 2];
     z[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
   }
-  const double z0 = z[0], z1 = z[1];
-  double u = (b2 ? z1 : z0) + __shfl_xor_sync(0xffffffffu, b2 ? z0 : z1, 4);
+  float u = (b2 ? z[1] : z[0]) + __shfl_xor_sync(0xffffffffu, b2 ? z[0] : z[1], 4);
   u += __shfl_xor_sync(0xffffffffu, u, 2);
   u += __shfl_xor_sync(0xffffffffu, u, 1);
-  if ((lane & 3) == 0) sacc[((unsigned long long)slot * nwarps + warp) * 8 + (lane >> 2)] += u;
+  if ((lane & 3) == 0) sacc[((unsigned long long)slot * nwarps + warp) * 8 + (lane >> 2)] += (double)u;
 }
 
 template <int TB, int CB, int KIND>
