@@ -22,7 +22,7 @@
 namespace vqc {
 
 int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vqc_pauli* terms, int nterms,
-              bool write, bool acc, bool hermitian_part, double* result);
+              bool write, bool acc, bool hermitian_part, double* result, bool* deferred = nullptr);
 int expect_dense_device(vqc_state h, const void* bra, const void* ket, int k, const int* sp, const std::vector<cd>& M,
                         double* res);
 int apply_circuit_raw(vqc_state h, const vqc_gate* gates, int ngates, const double* mats, bool dm, int fuse);
@@ -253,9 +253,18 @@ int vqc_adjoint_grad(vqc_state psi0, const vqc_gate* gates, int ngates, const do
   rc = apply_circuit_raw(psi0, gates, ngates, mats, false, 1);
   psi0->d = keep;
   if (rc) return rc;
-  // E = <y|H|y>; cotangent lam = (conj(z) H + z H^dagger) y with z = 1
-  if ((rc = pauli_run(psi0, y, y, lam, terms, nterms, true, true, true, energy))) return rc;
-  return reverse_sweep(psi0, lam, y, gates, ngates, mats, params, nparams, grads, true);
+  // E = <y|H|y>; cotangent lam = (conj(z) H + z H^dagger) y with z = 1.  E
+  // arrives after the reverse sweep, so that its planning on the host runs
+  // while the device is still busy with the forward passes.
+  bool deferred = false;
+  if ((rc = pauli_run(psi0, y, y, lam, terms, nterms, true, true, true, energy, &deferred))) return rc;
+  if ((rc = reverse_sweep(psi0, lam, y, gates, ngates, mats, params, nparams, grads, true))) return rc;
+  if (deferred) {
+    VQC_CK(cudaStreamSynchronize(psi0->stream));
+    energy[0] = psi0->h_result[kDeferredSlot];
+    energy[1] = psi0->h_result[kDeferredSlot + 1];
+  }
+  return VQC_OK;
 }
 
 int vqc_circuit_backward(vqc_state y, vqc_state delta, const vqc_gate* gates, int ngates, const double* mats,

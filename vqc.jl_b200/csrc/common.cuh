@@ -88,6 +88,10 @@ const DeviceInfo& device_info(int device);
 // (and result) does not change from call to call.
 constexpr int kRedThreads = 256;
 constexpr int kMaxAcc = 64;  // doubles reduced per launch
+// The last two doubles of a handle's pinned result buffer receive a result
+// copied without waiting (the gradient's energy, read after the reverse
+// sweep); fetch_result never reaches them.
+constexpr int kDeferredSlot = kMaxAcc - 2;
 int reduction_grid(int device, int64_t work_items);
 
 // ----------------------------------------------------------------------------- scratch

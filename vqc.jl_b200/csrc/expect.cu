@@ -264,7 +264,8 @@ int axpy_device(vqc_state h, void* y, const void* x) {
 // Runs the Pauli kernel in chunks of at most kMaxTermsPerLaunch terms; the
 // expectation (if any) is summed on the host in FP64 over chunks.
 int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vqc_pauli* terms, int nterms,
-              bool write, bool acc, bool hermitian_part, double* result) {
+              bool write, bool acc, bool hermitian_part, double* result, bool* deferred = nullptr) {
+  if (deferred) *deferred = false;
   double tot[2] = {0, 0};
   bool first = true;
   int start = 0;
@@ -349,14 +350,22 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
       if ((rc = axpy_device(h, out, target))) return rc;
     }
     if (acc) {
-      if ((rc = fetch_result(h, 2))) return rc;
-      tot[0] += h->h_result[0];
-      tot[1] += h->h_result[1];
+      if (deferred && first && start + cnt >= nterms) {
+        // one chunk: copy the sums to the handle's reserved pinned slot
+        // without waiting; the caller reads them after its next synchronisation
+        VQC_CK(cudaMemcpyAsync(h->h_result + kDeferredSlot, h->scr.result, 2 * sizeof(double),
+                               cudaMemcpyDeviceToHost, h->stream));
+        *deferred = true;
+      } else {
+        if ((rc = fetch_result(h, 2))) return rc;
+        tot[0] += h->h_result[0];
+        tot[1] += h->h_result[1];
+      }
     }
     first = false;
     start += cnt;
   } while (start < nterms);
-  if (result) {
+  if (result && !(deferred && *deferred)) {
     result[0] = tot[0];
     result[1] = tot[1];
   }

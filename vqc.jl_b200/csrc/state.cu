@@ -155,6 +155,7 @@ static void prof_collect() {
 }
 
 int fetch_result(vqc_state h, int n) {
+  if (n > kDeferredSlot) return fail(VQC_ERR_ARG, "internal: result fetch beyond the reserved slot");
   VQC_CK(cudaMemcpyAsync(h->h_result, h->scr.result, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
   VQC_CK(cudaStreamSynchronize(h->stream));
   return VQC_OK;
