@@ -159,6 +159,89 @@ def pauli_fixture(rng):
             "coeff": np.array(cs), "energy": e, "hpsi": hpsi}
 
 
+def _kraus2(rng):
+    A = [rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4)) for _ in range(3)]
+    S = sum(a.conj().T @ a for a in A)
+    w, U = np.linalg.eigh(S)
+    return [a @ (U @ np.diag(w ** -0.5) @ U.conj().T) for a in A]
+
+
+def noisy_dm_fixture(rng):
+    """A noisy circuit on a density matrix (channels: apply_qmaps.jl; the DM
+    pullback: circuitdiff.jl:35-75; tr(H rho): expecs_dm.jl), checked against
+    dense NumPy (sum_i K_i rho K_i^dagger, U rho U^dagger, tr(H rho)) and the
+    gradient against central differences of real(tr(H rho_out))."""
+    import vqcb200 as V
+    n = 4
+    N = 1 << n
+    psi = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    psi /= np.linalg.norm(psi)
+    th = rng.uniform(0, 2 * np.pi, 3 * n - 1)
+
+    def items_of(t):
+        its, k = [], 0
+        for q in range(n):
+            g = V.U3Gate(q + 1, t[k], 0.3, -0.2, isparas=[True, False, False])
+            its.append(("gate", [q], g.mat, g.derivatives()))
+            k += 1
+        its.append(("map", [1], V.Depolarizing(2, 0.15).kraus))
+        for q in range(n - 1):
+            g = V.CRxGate(q + 1, q + 2, t[k], isparas=True)
+            its.append(("gate", [q, q + 1], g.mat, g.derivatives()))
+            k += 1
+        its.append(("map", [3, 0], K2))
+        for q in range(n):
+            g = V.RyGate(q + 1, t[k], isparas=True)
+            its.append(("gate", [q], g.mat, g.derivatives()))
+            k += 1
+        its.append(("map", [2], V.AmplitudeDamping(3, 0.25).kraus))
+        return its
+
+    K2 = _kraus2(rng)
+    spec = [(0.36, {1: "X", 4: "Y"}), (0.7, {2: "Z"}), (-0.5, {1: "Z", 3: "X"}), (0.2, {2: "Y", 3: "Y"})]
+    terms = O.terms_from_spec(spec)
+    H = D.pauli_sum_matrix(n, terms)
+
+    def forward(t):
+        rho = O.density_matrix(psi)
+        R = rho.reshape(N, N, order="F").copy()
+        for kind, pos, *rest in items_of(t):
+            if kind == "map":
+                rho = O.dm_apply_channel(rho, n, pos, rest[0])
+                R = sum(D.full_operator(n, pos, K) @ R @ D.full_operator(n, pos, K).conj().T for K in rest[0])
+            else:
+                O.dm_apply_gate(rho, n, pos, rest[0])
+                Uf = D.full_operator(n, pos, rest[0])
+                R = Uf @ R @ Uf.conj().T
+            assert np.abs(rho - R.reshape(-1, order="F")).max() < 1e-12
+        return rho
+
+    rho = forward(th)
+    e = O.dm_expectation(terms, rho, n)
+    assert abs(e - np.trace(H @ rho.reshape(N, N, order="F"))) < 1e-12
+    its = items_of(th)
+    g, d_in, y_in = O.dm_circuit_gradient(its, rho, H.conj().T.reshape(-1, order="F").copy(), n)
+    assert np.abs(y_in - O.density_matrix(psi)).max() < 1e-10
+    h = 1e-4
+    fd = np.array([(O.dm_expectation(terms, forward(th + h * u), n).real -
+                    O.dm_expectation(terms, forward(th - h * u), n).real) / (2 * h) for u in np.eye(th.size)])
+    assert np.abs(g - fd).max() < 1e-6
+    out = {"n": n, "psi": psi, "theta": th, "kraus2": np.array(K2), "rho": rho, "energy": e, "grads": g,
+           "delta_in": d_in, "nitems": len(its),
+           "xmask": np.array([sum(1 << (q - 1) for q, o in ops.items() if o in "XY") for _, ops in spec], np.uint64),
+           "zmask": np.array([sum(1 << (q - 1) for q, o in ops.items() if o in "ZY") for _, ops in spec], np.uint64),
+           "coeff": np.array([c for c, _ in spec], dtype=complex)}
+    for i, (kind, pos, *rest) in enumerate(its):
+        out["kind%d" % i] = np.array(0 if kind == "gate" else 1)
+        out["pos%d" % i] = np.array(pos)
+        if kind == "gate":
+            out["mat%d" % i] = rest[0]
+            out["der%d" % i] = np.array(rest[1]) if rest[1] else np.zeros((0, 1 << len(pos), 1 << len(pos)))
+        else:
+            out["kraus%d" % i] = np.array(rest[0])
+    return out
+
+
 FIXTURES = {
     "gates_n7": gates_fixture,
     "hea_tfim_n12": hea_fixture,
@@ -166,11 +249,15 @@ FIXTURES = {
     "u3_cz_toffoli_n10": u3cz_fixture,
     "dm_u3_cnot_n5": dm_fixture,
     "pauli_sum_n9": pauli_fixture,
+    "noisy_dm_n4": noisy_dm_fixture,
 }
 
 
-def main():
+def main(names=None):
+    """Writes every fixture, or only the named ones (python make_golden.py NAME...)."""
     for i, (name, fn) in enumerate(FIXTURES.items()):
+        if names and name not in names:
+            continue
         rng = np.random.default_rng(20261203 + i)
         d = fn(rng)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **d)
@@ -178,4 +265,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

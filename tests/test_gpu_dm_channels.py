@@ -152,3 +152,56 @@ def test_noisy_dm_gradient(dtype, loss):
     assert np.abs(g - g_ref).max() < (1e-10 if dtype == np.complex128 else 5e-5) * scale
     assert max_abs(y.data(), y_ref) < tol(dtype) * 100
     assert max_abs(d.data(), d_ref) < tol(dtype) * 100 * max(1.0, np.abs(d_ref).max())
+
+
+def _golden_noisy_items(d):
+    """The fixture's noisy circuit, built from its parameters with the
+    package's gate and channel constructors (item order as generated)."""
+    n, th = int(d["n"]), d["theta"]
+    items, k = [], 0
+    for q in range(1, n + 1):
+        items.append(V.U3Gate(q, float(th[k]), 0.3, -0.2, isparas=[True, False, False]))
+        k += 1
+    items.append(V.Depolarizing(2, 0.15))
+    for q in range(1, n):
+        items.append(V.CRxGate(q, q + 1, float(th[k]), isparas=True))
+        k += 1
+    items.append(V.QuantumMap((4, 1), list(d["kraus2"])))
+    for q in range(1, n + 1):
+        items.append(V.RyGate(q, float(th[k]), isparas=True))
+        k += 1
+    items.append(V.AmplitudeDamping(3, 0.25))
+    return items
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_golden_noisy_dm(dtype):
+    """Committed fixture (oracle, checked against dense NumPy and central
+    differences when generated): noisy circuit on a density matrix, tr(H rho)
+    and the DM pullback (apply_qmaps.jl, expecs_dm.jl, circuitdiff.jl:42-75)."""
+    from helpers import golden
+    d = golden("noisy_dm_n4")
+    n = int(d["n"])
+    items = _golden_noisy_items(d)
+    assert len(items) == int(d["nitems"])
+    for i, it in enumerate(items):
+        if int(d["kind%d" % i]) == 0:
+            assert np.abs(it.mat - d["mat%d" % i]).max() < 1e-14
+    rho = V.DensityMatrix(V.StateVector(d["psi"].astype(dtype), dtype=dtype))
+    c = V.QCircuit(items)
+    V.apply(c, rho)
+    assert max_abs(rho.data(), d["rho"]) < tol(dtype) * 10
+    H = V.QubitsOperator(*[V.QubitsTerm({q + 1: "IXZY"[((int(x) >> q) & 1) | (((int(z) >> q) & 1) << 1)]
+                                          for q in range(n) if ((int(x) | int(z)) >> q) & 1}, coeff=complex(cf))
+                            for x, z, cf in zip(d["xmask"], d["zmask"], d["coeff"])])
+    e = V.expectation(H, rho)
+    assert abs(e - d["energy"]) < tol(dtype) * 10
+    terms = [O.make_term({q: "IXZY"[((int(x) >> q) & 1) | (((int(z) >> q) & 1) << 1)]
+                          for q in range(n) if ((int(x) | int(z)) >> q) & 1}, complex(cf))
+             for x, z, cf in zip(d["xmask"], d["zmask"], d["coeff"])]
+    dmat = D.pauli_sum_matrix(n, terms).conj().T
+    delta = V.DensityMatrix(dmat.astype(dtype), dtype=dtype)
+    dd, g, _ = V.back_propagate(delta, c, rho)
+    scale = max(1.0, np.abs(d["grads"]).max())
+    assert np.abs(g - d["grads"]).max() < (1e-10 if dtype == np.complex128 else 5e-5) * scale
+    assert max_abs(dd.data(), d["delta_in"]) < tol(dtype) * 100 * max(1.0, np.abs(d["delta_in"]).max())

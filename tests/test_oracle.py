@@ -157,6 +157,30 @@ def test_golden_fixtures_reproduce():
     for i in range(int(d["ncases"])):
         out = O.apply_gate(d["psi"].copy(), list(d["pos%d" % i]), d["U%d" % i])
         assert max_abs(out, d["out%d" % i]) < 1e-13
+    d = golden("noisy_dm_n4")
+    n = int(d["n"])
+    items = []
+    for i in range(int(d["nitems"])):
+        pos = [int(p) for p in d["pos%d" % i]]
+        if int(d["kind%d" % i]) == 1:
+            items.append(("map", pos, list(d["kraus%d" % i])))
+        else:
+            items.append(("gate", pos, d["mat%d" % i], list(d["der%d" % i])))
+    rho = O.density_matrix(d["psi"])
+    for it in items:
+        if it[0] == "map":
+            rho = O.dm_apply_channel(rho, n, it[1], it[2])
+        else:
+            O.dm_apply_gate(rho, n, it[1], it[2])
+    assert max_abs(rho, d["rho"]) < 1e-13
+    terms = [O.make_term({q: o for q, o in enumerate("IXZY"[((int(x) >> q) & 1) | (((int(z) >> q) & 1) << 1)]
+                                                     for q in range(n)) if o != "I"}, complex(c))
+             for x, z, c in zip(d["xmask"], d["zmask"], d["coeff"])]
+    assert abs(O.dm_expectation(terms, rho, n) - d["energy"]) < 1e-13
+    H = D.pauli_sum_matrix(n, terms)
+    g, d_in, _ = O.dm_circuit_gradient(items, rho, H.conj().T.reshape(-1, order="F").copy(), n)
+    assert np.abs(g - d["grads"]).max() < 1e-12
+    assert max_abs(d_in, d["delta_in"]) < 1e-12
 
 
 def test_oracle_rejects_bad_positions():
