@@ -910,6 +910,20 @@ static int acc_kind(const FOp& f) {
   if (off && !diag) return kAccOff;
   return kAccFull;
 }
+// Every D of the op anti-Hermitian (as U^dagger dU/dtheta of a unitary family
+// is): the FP32 body then accumulates the four-value projection (kAccAH).
+static bool acc_anti_hermitian(const FOp& f) {
+  for (const PGrad& pg : f.grads) {
+    if (pg.D.size() != 4) return false;
+    double scale = 0;
+    for (const cd& d : pg.D) scale = std::max(scale, std::abs(d));
+    const double eps = 1e-12 * scale;
+    if (std::abs(pg.D[0].real()) > eps || std::abs(pg.D[3].real()) > eps ||
+        std::abs(pg.D[1] + std::conj(pg.D[2])) > eps)
+      return false;
+  }
+  return !f.grads.empty();
+}
 
 // One stage of the FP32 (packed) tile body: its DevStageF tables, its ops
 // (j-bit targets, register controls as compile-time cases or a mask, the
@@ -994,7 +1008,7 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
     if (f.kind == kOpU1) {
       const int tb = jbit(tbit[f.tq[0]]), form = u1_form(f.mat);
       o.code |= (tb << 4) | (form << 11) | (rctl << 16);
-      if (adj && f.acc) o.code |= acc_kind(f) << 14;
+      if (adj && f.acc) o.code |= (acc_kind(f) << 14) | (acc_anti_hermitian(f) ? kCodeAH : 0);
       const cd u00 = f.mat[0], u01 = f.mat[1], u10 = f.mat[2], u11 = f.mat[3];
       if (tb != 0) {
         switch (form) {
@@ -1054,7 +1068,7 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
         if (accs) accs->push_back(AccRef{row + o.slot, f});
         continue;
       }
-      if (accs) accs->push_back(AccRef{row + o.slot, f});
+      if (accs) accs->push_back(AccRef{row + o.slot, f, (o.code & kCodeAH) != 0});
       o.code |= kCodeAcc;
     }
     dops.push_back(o);
@@ -1512,6 +1526,13 @@ namespace vqc {
 void contract_grads(const std::vector<AccRef>& accs, const double* A, double* grads) {
   for (const AccRef& a : accs) {
     const double* r = &A[(size_t)a.row * 8];
+    if (a.ah) {
+      // r = (Im A00, Im A11, Re A01 - Re A10, Im A01 + Im A10), D anti-Hermitian
+      for (const PGrad& pg : a.op.grads)
+        grads[pg.param] = -pg.D[0].imag() * r[0] - pg.D[3].imag() * r[1] + pg.D[1].real() * r[2] -
+                          pg.D[1].imag() * r[3];
+      continue;
+    }
     const cd Av[4] = {cd(r[0], r[1]), cd(r[2], r[3]), cd(r[4], r[5]), cd(r[6], r[7])};
     for (const PGrad& pg : a.op.grads) {
       double g = 0;

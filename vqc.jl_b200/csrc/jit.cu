@@ -128,7 +128,7 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o) {
   os << "    { const DevOp* op = x.ops + " << o << ";\n";
   if (gctl) os << "      if ((x.base & op->gmask) == op->gval) {\n";
   if (type == kOpU1) {
-    const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = (code >> 14) & 3;
+    const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = acc_kind_of(code);
     const int cb = rctl == 0 ? -1 : rctl - 1;
     os << "      const u64* c = coef.c + " << op.mat << ";\n";
     if (ctl) os << "      const bool run = (tthr & op->cmask) == op->cval;\n";
@@ -145,7 +145,7 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o) {
         os << "        acc_static<" << tb << ", " << cb << ", " << kind << ">(v, w, s8);\n";
     }
     os << "      }\n";
-    if (acc) os << "      flush8(s8, x.sacc, op->slot, NW);\n";
+    if (acc) os << "      " << ((kind & kAccAH) ? "flush4" : "flush8") << "(s8, x.sacc, op->slot, NW);\n";
   } else if (type == kOpU2) {
     const int ja = (code >> 4) & 3, jb = (code >> 6) & 3;
     if (ctl) os << "      if ((tthr & op->cmask) == op->cval)\n";

@@ -69,13 +69,20 @@ struct alignas(16) DevOp {
   int32_t rmask;    // FP32 body: register amplitudes (pair representatives) the controls enable
 };
 constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
-// bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries accumulated
+// bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries
+// accumulated; bits 16-18: register control; bit 19: anti-Hermitian projection
+constexpr int kCodeAH = 1 << 19;
 // One-qubit matrix forms (read off the matrix on the host): general complex;
 // "RI" = real diagonal and imaginary off-diagonal (RX-like); real (RY-like);
 // diagonal (RZ / phase); the exact swap [[0,1],[1,0]] (X, the CNOT/Toffoli target).
 enum { kFormGen = 0, kFormRI = 1, kFormReal = 2, kFormDiag = 3, kFormSwap = 4 };
-// Reduced-matrix entries a parameter's D touches: all four, off-diagonal, diagonal.
-enum { kAccFull = 0, kAccOff = 1, kAccDiag = 2 };
+// Reduced-matrix entries a parameter's D touches: all four, off-diagonal,
+// diagonal; kAccAH added (FP32 body) when every D is anti-Hermitian and only
+// (Im A00, Im A11, Re A01 - Re A10, Im A01 + Im A10) are accumulated.
+enum { kAccFull = 0, kAccOff = 1, kAccDiag = 2, kAccAH = 4 };
+__host__ __device__ constexpr int acc_kind_of(int code) {
+  return ((code >> 14) & 3) | ((code & kCodeAH) ? kAccAH : 0);
+}
 
 // Shared-memory bytes of the FP32 tile(s) of one pass.
 template <int M, bool ADJ>

@@ -302,6 +302,59 @@ __device__ __forceinline__ void acc_lane(u64 (&c)[4], const Pk& L, const Pk& P) 
     c[3] = fma2(L.r, qi, fma2(ni, qr, c[3]));
   }
 }
+// Anti-Hermitian projection (KIND & kAccAH): when every matrix D the op's
+// partials contract with is anti-Hermitian (D = U^dagger dU/dtheta of a
+// unitary family), Re sum_ab D_ab A_ab = -Im D00 s0 - Im D11 s1 + Re D01 s2
+// - Im D01 s3 needs only s = (Im A00, Im A11, Re A01 - Re A10, Im A01 + Im A10):
+// three quarters of the products and half the values to reduce.
+template <int KIND>
+__device__ __forceinline__ void acch_free(u64 (&a)[5], const Pk& L0, const Pk& L1, const Pk& P0, const Pk& P1) {
+  const u64 n0i = neg2(L0.i), n1i = neg2(L1.i);
+  if ((KIND & 3) != kAccOff) {
+    a[0] = fma2(L0.r, P0.i, fma2(n0i, P0.r, a[0]));
+    a[1] = fma2(L1.r, P1.i, fma2(n1i, P1.r, a[1]));
+  }
+  if ((KIND & 3) != kAccDiag) {
+    a[2] = fma2(L0.r, P1.r, fma2(L0.i, P1.i, a[2]));
+    a[3] = fma2(L1.r, P0.r, fma2(L1.i, P0.i, a[3]));
+    a[4] = fma2(L0.r, P1.i, fma2(n0i, P1.r, fma2(L1.r, P0.i, fma2(n1i, P0.r, a[4]))));
+  }
+}
+template <int KIND, int LANE>
+__device__ __forceinline__ void acch_scalar(float (&s)[8], const Pk& L0, const Pk& L1, const Pk& P0, const Pk& P1) {
+  const float l0r = LANE ? hi(L0.r) : lo(L0.r), l0i = LANE ? hi(L0.i) : lo(L0.i);
+  const float l1r = LANE ? hi(L1.r) : lo(L1.r), l1i = LANE ? hi(L1.i) : lo(L1.i);
+  const float p0r = LANE ? hi(P0.r) : lo(P0.r), p0i = LANE ? hi(P0.i) : lo(P0.i);
+  const float p1r = LANE ? hi(P1.r) : lo(P1.r), p1i = LANE ? hi(P1.i) : lo(P1.i);
+  if ((KIND & 3) != kAccOff) {
+    s[0] = fmaf(l0r, p0i, fmaf(-l0i, p0r, s[0]));
+    s[1] = fmaf(l1r, p1i, fmaf(-l1i, p1r, s[1]));
+  }
+  if ((KIND & 3) != kAccDiag) {
+    s[2] = fmaf(l0r, p1r, fmaf(l0i, p1i, fmaf(-l1r, p0r, fmaf(-l1i, p0i, s[2]))));
+    s[3] = fmaf(l0r, p1i, fmaf(-l0i, p1r, fmaf(l1r, p0i, fmaf(-l1i, p0r, s[3]))));
+  }
+}
+// lane target: c0 = (Im A00, Im A11), c1 = (Re A01, Re A10), c2 = (Im A01, Im A10)
+template <int KIND>
+__device__ __forceinline__ void acch_lane(u64 (&c)[3], const Pk& L, const Pk& P) {
+  const u64 ni = neg2(L.i);
+  if ((KIND & 3) != kAccOff) c[0] = fma2(L.r, P.i, fma2(ni, P.r, c[0]));
+  if ((KIND & 3) != kAccDiag) {
+    const u64 qr = swp(P.r), qi = swp(P.i);
+    c[1] = fma2(L.r, qr, fma2(L.i, qi, c[1]));
+    c[2] = fma2(L.r, qi, fma2(ni, qr, c[2]));
+  }
+}
+__device__ __forceinline__ void packh_free(const u64 (&a)[5], float (&s)[8]) {
+  s[0] = lo(a[0]) + hi(a[0]);
+  s[1] = lo(a[1]) + hi(a[1]);
+  s[2] = (lo(a[2]) + hi(a[2])) - (lo(a[3]) + hi(a[3]));
+  s[3] = lo(a[4]) + hi(a[4]);
+}
+__device__ __forceinline__ void packh_lane(const u64 (&c)[3], float (&s)[8]) {
+  s[0] = lo(c[0]), s[1] = hi(c[0]), s[2] = lo(c[1]) - hi(c[1]), s[3] = lo(c[2]) + hi(c[2]);
+}
 __device__ __forceinline__ void pack_free(const u64 (&a)[8], float (&s)[8]) {
 #pragma unroll
   for (int i = 0; i < 8; ++i) s[i] = lo(a[i]) + hi(a[i]);
@@ -337,9 +390,52 @@ __device__ __forceinline__ void flush8(const float (&s)[8], double* sacc, int sl
   if ((lane & 3) == 0) sacc[((unsigned long long)slot * nwarps + warp) * 8 + (lane >> 2)] += (double)u;
 }
 
+// The first four values only (an anti-Hermitian projection); lane L with
+// L % 8 == 0 holds the warp total of value L / 8 afterwards.
+__device__ __forceinline__ void flush4(const float (&s)[8], double* sacc, int slot, int nwarps) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool b4 = lane & 16, b3 = lane & 8;
+  float y[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float keep = b4 ? s[i + 2] : s[i], send = b4 ? s[i] : s[i + 2];
+    y[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  float u = (b3 ? y[1] : y[0]) + __shfl_xor_sync(0xffffffffu, b3 ? y[0] : y[1], 8);
+  u += __shfl_xor_sync(0xffffffffu, u, 4);
+  u += __shfl_xor_sync(0xffffffffu, u, 2);
+  u += __shfl_xor_sync(0xffffffffu, u, 1);
+  if ((lane & 7) == 0) sacc[((unsigned long long)slot * nwarps + warp) * 8 + (lane >> 3)] += (double)u;
+}
+
 template <int TB, int CB, int KIND>
 __device__ __forceinline__ void acc_static(const Pk (&v)[8], const Pk (&w)[8], float (&s8)[8]) {
-  if constexpr (TB == 0) {
+  if constexpr ((KIND & kAccAH) && TB == 0) {
+    u64 c[3] = {0, 0, 0};
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      if (CB > 0 && !((m >> (CB - 1)) & 1)) continue;
+      acch_lane<KIND>(c, w[m], v[m]);
+    }
+    packh_lane(c, s8);
+  } else if constexpr ((KIND & kAccAH) && CB == 0) {
+    constexpr int T = TB - 1;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const int m0 = ((g >> T) << (T + 1)) | (g & ((1 << T) - 1)), m1 = m0 | (1 << T);
+      acch_scalar<KIND, 1>(s8, w[m0], w[m1], v[m0], v[m1]);
+    }
+  } else if constexpr (KIND & kAccAH) {
+    constexpr int T = TB - 1;
+    u64 a[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const int m0 = ((g >> T) << (T + 1)) | (g & ((1 << T) - 1)), m1 = m0 | (1 << T);
+      if (CB > 0 && !((m0 >> (CB - 1)) & 1)) continue;
+      acch_free<KIND>(a, w[m0], w[m1], v[m0], v[m1]);
+    }
+    packh_free(a, s8);
+  } else if constexpr (TB == 0) {
     u64 c[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
@@ -368,7 +464,21 @@ __device__ __forceinline__ void acc_static(const Pk (&v)[8], const Pk (&w)[8], f
 }
 template <int TB, int KIND>
 __device__ __forceinline__ void acc_masked(const Pk (&v)[8], const Pk (&w)[8], uint32_t rmask, float (&s8)[8]) {
-  if constexpr (TB == 0) {
+  if constexpr ((KIND & kAccAH) && TB == 0) {
+    u64 c[3] = {0, 0, 0};
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+      if ((rmask >> (2 * m)) & 1) acch_lane<KIND>(c, w[m], v[m]);
+    packh_lane(c, s8);
+  } else if constexpr (KIND & kAccAH) {
+    constexpr int T = TB - 1;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const int m0 = ((g >> T) << (T + 1)) | (g & ((1 << T) - 1)), m1 = m0 | (1 << T);
+      if ((rmask >> (2 * m0)) & 1) acch_scalar<KIND, 0>(s8, w[m0], w[m1], v[m0], v[m1]);
+      if ((rmask >> (2 * m0 + 1)) & 1) acch_scalar<KIND, 1>(s8, w[m0], w[m1], v[m0], v[m1]);
+    }
+  } else if constexpr (TB == 0) {
     u64 c[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int m = 0; m < 8; ++m)
@@ -411,6 +521,9 @@ __device__ __forceinline__ void acc_kind(int kind, const Pk (&v)[8], const Pk (&
   switch (kind) {
     case kAccOff: acc_static<TB, CB, kAccOff>(v, w, s8); break;
     case kAccDiag: acc_static<TB, CB, kAccDiag>(v, w, s8); break;
+    case kAccAH | kAccFull: acc_static<TB, CB, kAccAH | kAccFull>(v, w, s8); break;
+    case kAccAH | kAccOff: acc_static<TB, CB, kAccAH | kAccOff>(v, w, s8); break;
+    case kAccAH | kAccDiag: acc_static<TB, CB, kAccAH | kAccDiag>(v, w, s8); break;
     default: acc_static<TB, CB, kAccFull>(v, w, s8); break;
   }
 }
@@ -420,6 +533,9 @@ __device__ __forceinline__ void acc_kind_masked(int kind, const Pk (&v)[8], cons
   switch (kind) {
     case kAccOff: acc_masked<TB, kAccOff>(v, w, rmask, s8); break;
     case kAccDiag: acc_masked<TB, kAccDiag>(v, w, rmask, s8); break;
+    case kAccAH | kAccFull: acc_masked<TB, kAccAH | kAccFull>(v, w, rmask, s8); break;
+    case kAccAH | kAccOff: acc_masked<TB, kAccAH | kAccOff>(v, w, rmask, s8); break;
+    case kAccAH | kAccDiag: acc_masked<TB, kAccAH | kAccDiag>(v, w, rmask, s8); break;
     default: acc_masked<TB, kAccFull>(v, w, rmask, s8); break;
   }
 }
@@ -797,7 +913,7 @@ __device__ __forceinline__ void interp_ops(const TileCtx<M, ADJ>& x, const DevSt
     if (!GEN || type == kOpU1) {
       const bool acc = ADJ && (code & kCodeAcc);
       if (!run && !acc) continue;
-      const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = (code >> 14) & 3;
+      const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = acc_kind_of(code);
       const uint32_t rmask = (uint32_t)op->rmask;
       float s8[8];
 #pragma unroll
@@ -810,7 +926,12 @@ __device__ __forceinline__ void interp_ops(const TileCtx<M, ADJ>& x, const DevSt
           default: u1_target<3, ADJ>(rctl, form, acc, kind, rmask, v, w, c2, s8); break;
         }
       }
-      if (ADJ && acc) flush8(s8, x.sacc, op->slot, NW);
+      if (ADJ && acc) {
+        if (kind & kAccAH)
+          flush4(s8, x.sacc, op->slot, NW);
+        else
+          flush8(s8, x.sacc, op->slot, NW);
+      }
     } else if (!run && type != kOpAccD) {  // (diagonal ops carry no controls; AccD always reduces)
     } else if (type == kOpU2) {
       u2_dispatch<ADJ>((code >> 4) & 3, (code >> 6) & 3, v, w, c, (uint32_t)op->rmask);

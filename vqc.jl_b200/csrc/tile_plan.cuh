@@ -63,6 +63,7 @@ struct PassShape {
 struct AccRef {
   int row;
   FOp op;
+  bool ah = false;  // the row holds the anti-Hermitian projection (kAccAH)
 };
 
 struct PassLoc {
