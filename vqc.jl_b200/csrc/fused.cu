@@ -627,7 +627,9 @@ static TileConfig tile_config(int dtype, int n) {
   // 2^12 FP32 or 2^11 FP64 amplitudes per tile (32 KiB per state), smaller
   // tiles for smaller states; the lowest 4 (FP32) / 3 (FP64) qubits are always
   // tile qubits so that a tile is made of 128-byte runs (11-qubit FP32 tiles
-  // for the reverse sweep measured slower: more passes at the same pass cost)
+  // for the reverse sweep measured slower: more passes at the same pass cost;
+  // 3 always-resident FP32 qubits give 10 % fewer passes at 1.4x the reverse
+  // pass time, 11.6 vs 12.6 gradients/s at n = 26)
   const int M = std::min(dtype == VQC_C64 ? 12 : 11, n);
   return {M, std::min(dtype == VQC_C64 ? 4 : 3, M)};
 }
