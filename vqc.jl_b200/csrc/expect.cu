@@ -114,28 +114,39 @@ struct DevGroup4 {
   int pad;
 };
 
-template <int AX>
-__device__ __forceinline__ void pauli4_add(double2 (&hv)[4], const double2 (&W)[4], const double2 (&kv)[4]) {
+// The quad kernel computes in the state's precision (FP32 phases and
+// products for FP32 states, whose written output is FP32); the expectation
+// itself is accumulated in FP64.  The class sums F of real Pauli-sum
+// coefficients such as 1 and 0.5 are exact in either precision.
+template <class R>
+struct PTerm {
+  uint64_t z;
+  cplx<R> c, d;
+};
+template <int AX, class V>
+__device__ __forceinline__ void pauli4_add(V (&hv)[4], const V (&W)[4], const V (&kv)[4]) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) hv[a] = cfma(W[a ^ AX], kv[a ^ AX], hv[a]);
 }
-__device__ __forceinline__ void pauli4_wh(const double2 (&F)[4], double2 (&W)[4]) {
-  const double2 s01 = make_double2(F[0].x + F[1].x, F[0].y + F[1].y), d01 = make_double2(F[0].x - F[1].x, F[0].y - F[1].y);
-  const double2 s23 = make_double2(F[2].x + F[3].x, F[2].y + F[3].y), d23 = make_double2(F[2].x - F[3].x, F[2].y - F[3].y);
-  W[0] = make_double2(s01.x + s23.x, s01.y + s23.y);
-  W[1] = make_double2(d01.x + d23.x, d01.y + d23.y);
-  W[2] = make_double2(s01.x - s23.x, s01.y - s23.y);
-  W[3] = make_double2(d01.x - d23.x, d01.y - d23.y);
+template <class V>
+__device__ __forceinline__ void pauli4_wh(const V (&F)[4], V (&W)[4]) {
+  V s01, d01, s23, d23;
+  s01.x = F[0].x + F[1].x, s01.y = F[0].y + F[1].y, d01.x = F[0].x - F[1].x, d01.y = F[0].y - F[1].y;
+  s23.x = F[2].x + F[3].x, s23.y = F[2].y + F[3].y, d23.x = F[2].x - F[3].x, d23.y = F[2].y - F[3].y;
+  W[0].x = s01.x + s23.x, W[0].y = s01.y + s23.y;
+  W[1].x = d01.x + d23.x, W[1].y = d01.y + d23.y;
+  W[2].x = s01.x - s23.x, W[2].y = s01.y - s23.y;
+  W[3].x = d01.x - d23.x, W[3].y = d01.y - d23.y;
 }
 template <class R>
-__device__ __forceinline__ void load4(const cplx<R>* p, double2 (&kv)[4]) {
+__device__ __forceinline__ void load4(const cplx<R>* p, cplx<R> (&kv)[4]) {
   if constexpr (sizeof(R) == 4) {
     const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 2);
-    kv[0] = make_double2(a.x, a.y), kv[1] = make_double2(a.z, a.w);
-    kv[2] = make_double2(b.x, b.y), kv[3] = make_double2(b.z, b.w);
+    kv[0] = make_float2(a.x, a.y), kv[1] = make_float2(a.z, a.w);
+    kv[2] = make_float2(b.x, b.y), kv[3] = make_float2(b.z, b.w);
   } else {
 #pragma unroll
-    for (int b = 0; b < 4; ++b) kv[b] = to_d2(p[b]);
+    for (int b = 0; b < 4; ++b) kv[b] = p[b];
   }
 }
 
@@ -144,42 +155,47 @@ __global__ void __launch_bounds__(kRedThreads)
     k_pauli4(const cplx<R>* __restrict__ bra, const cplx<R>* __restrict__ ket, cplx<R>* __restrict__ out, int64_t N,
              const DevGroup4* __restrict__ groups, int ng, const DevTerm* __restrict__ terms, int nt, double dfac,
              Scratch s, double* res) {
+  using V = cplx<R>;
   extern __shared__ unsigned char smem[];
   DevGroup4* sg = reinterpret_cast<DevGroup4*>(smem);
-  DevTerm* st = reinterpret_cast<DevTerm*>(smem + sizeof(DevGroup4) * ng);
+  PTerm<R>* st = reinterpret_cast<PTerm<R>*>(smem + sizeof(DevGroup4) * ng);
   for (int i = threadIdx.x; i < ng; i += blockDim.x) sg[i] = groups[i];
-  for (int i = threadIdx.x; i < nt; i += blockDim.x) st[i] = terms[i];
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+    const DevTerm t = terms[i];
+    st[i] = PTerm<R>{t.z, mkc<R>((R)t.c.x, (R)t.c.y), mkc<R>((R)t.d.x, (R)t.d.y)};
+  }
   __syncthreads();
   double acc[2] = {0, 0};
+  const V zero = mkc<R>(R(0), R(0));
   const int64_t stride = (int64_t)gridDim.x * blockDim.x, nq4 = N >> 2;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nq4; k += stride) {
     const int64_t i0 = k << 2;
-    double2 hv[4], ov[4];
+    V hv[4], ov[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) hv[a] = ov[a] = make_double2(0, 0);
+    for (int a = 0; a < 4; ++a) hv[a] = ov[a] = zero;
     for (int gi = 0; gi < ng; ++gi) {
       const DevGroup4& g = sg[gi];
       const int64_t jb = i0 ^ (int64_t)(g.x & ~3ull);
-      double2 kv[4];
+      V kv[4];
       load4<R>(ket + jb, kv);
-      double2 F[4], Fd[4];
+      V F[4], Fd[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        F[c] = Fd[c] = make_double2(0, 0);
+        F[c] = Fd[c] = zero;
         for (int q = g.cs[c]; q < g.cs[c + 1]; ++q) {
           const uint64_t m = (uint64_t)jb & st[q].z;
           const bool odd = (__popc((unsigned)m ^ (unsigned)(m >> 32)) & 1) != 0;
-          const double2 cc = st[q].c;
+          const V cc = st[q].c;
           F[c].x += odd ? -cc.x : cc.x;
           F[c].y += odd ? -cc.y : cc.y;
           if (SEP) {
-            const double2 dd = st[q].d;
+            const V dd = st[q].d;
             Fd[c].x += odd ? -dd.x : dd.x;
             Fd[c].y += odd ? -dd.y : dd.y;
           }
         }
       }
-      double2 W[4], Wd[4];
+      V W[4], Wd[4];
       pauli4_wh(F, W);
       if (SEP) pauli4_wh(Fd, Wd);
       switch ((int)(g.x & 3)) {
@@ -190,19 +206,18 @@ __global__ void __launch_bounds__(kRedThreads)
       }
     }
     if (WRITE) {
+      const R df = (R)dfac;  // 1 or 2
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const double2 o = SEP ? ov[a] : make_double2(dfac * hv[a].x, dfac * hv[a].y);
-        out[i0 + a] = mkc<R>((R)o.x, (R)o.y);
-      }
+      for (int a = 0; a < 4; ++a) out[i0 + a] = SEP ? ov[a] : mkc<R>(df * hv[a].x, df * hv[a].y);
     }
     if (ACC) {
-      double2 b[4];
+      V b[4];
       load4<R>(bra + i0, b);
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        acc[0] = fma(b[a].x, hv[a].x, fma(b[a].y, hv[a].y, acc[0]));
-        acc[1] = fma(b[a].x, hv[a].y, fma(-b[a].y, hv[a].x, acc[1]));
+        const double2 bb = to_d2(b[a]), hh = to_d2(hv[a]);
+        acc[0] = fma(bb.x, hh.x, fma(bb.y, hh.y, acc[0]));
+        acc[1] = fma(bb.x, hh.y, fma(-bb.y, hh.x, acc[1]));
       }
     }
   }
