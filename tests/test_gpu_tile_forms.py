@@ -163,3 +163,43 @@ def test_f32_headline_shape(jit, monkeypatch):
     e64, g64 = V.energy_and_gradient(W.to_operator(hspec), W.to_circuit(spec), V.StateVector(n, dtype=np.complex128))
     assert abs(e - e64) / abs(e64) < tol(np.complex64) * 10
     assert rel(g, g64) < tol(np.complex64) * 10
+
+
+@pytest.mark.parametrize("jit", JIT)
+def test_f32_partials_not_anti_hermitian(jit, monkeypatch):
+    """Parameters whose D = U^dagger dU is not anti-Hermitian (dU supplied
+    freely: full, diagonal-only and off-diagonal-only D, a gate mixing such a
+    D with an anti-Hermitian one, and the same under a control on |0>) keep
+    the full reduced-matrix accumulation; unitary families take the
+    four-value anti-Hermitian projection.  Both against the oracle."""
+    monkeypatch.setenv("VQC_JIT", jit)
+    rng = np.random.default_rng(408)
+    Z = np.zeros((2, 2))
+    gates = []
+    for q in ONE_Q:
+        U = GR.random_unitary(1, rng)
+        Dfull = rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))
+        Ddiag = np.diag(rng.standard_normal(2))
+        Doff = np.array([[0, 0.6], [0.6, 0]])
+        Dah = -0.5j * np.array([[0, 1], [1, 0]])
+        gates += [
+            V.Gate((q,), U, (0.3,), True, [U @ Dfull], name="Dfull"),
+            V.Gate((q,), U, (0.2,), True, [U @ Ddiag], name="Ddiag"),
+            V.Gate((q,), U, (0.1,), True, [U @ Doff], name="Doff"),
+            V.Gate((q,), U, (0.4, 0.5), True, [U @ Dah, U @ Doff], name="Dmixed"),
+        ]
+        gates += one_qubit_gates(rng, q, True)[:4]
+    for c, t in PAIRS[:6]:
+        U = GR.random_unitary(1, rng)
+        Dfull = rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))
+        gates.append(V.Gate((c, t), _ctrl0(U), (0.7,), True, [_ctrl0(U @ Dfull) - _ctrl0(Z)], name="C0Dfull"))
+        gates += controlled_gates(rng, c, t, True)[:2]
+    gates = [gates[i] for i in rng.permutation(len(gates))]
+    c = V.QCircuit(gates)
+    psi0 = rand_psi(rng, N)
+    target = rand_psi(rng, N)
+    g_ref, d_ref = O.circuit_gradient(to_ref(gates), psi0, target, nthreads=4)
+    y = c * V.StateVector(psi0.astype(np.complex64), dtype=np.complex64)
+    delta, g, _ = V.back_propagate(V.StateVector(target.astype(np.complex64), dtype=np.complex64), c, y)
+    assert rel(g, g_ref) < 2e-5
+    assert max_abs(delta.storage(), d_ref) < 2e-5
