@@ -497,11 +497,14 @@ def run_serve(args, local_rank):
             th.join()
             st = srv.stats()
             tm = srv.timing()
+            lt = srv.loop_timing()
         lat = np.array(lat)
         return {"rate_offered": rate, "requests": count, "throughput": count / makespan,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "mean_batch": st["request_steps"] / max(st["launches"], 1), "loop_iterations": st["iterations"],
-                "phases_ms": {k: round(v * 1e3, 3) for k, v in tm.items()}}
+                "phases_ms": {k: round(v * 1e3, 3) for k, v in tm.items()},
+                "busy_iteration_ms": {(k if k == "iterations" else k[:-2]): (v if k == "iterations" else round(v * 1e3, 4))
+                                      for k, v in lt.items()}}
 
     # baseline: plain FP64, one request at a time, in arrival order
     def baseline(rate, count):

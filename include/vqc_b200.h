@@ -251,6 +251,11 @@ int vqc_serve_stats(vqc_server s, long long* out);
 /* out[0..5] (seconds): mean and max planning time, mean and max wait for
  * admission, mean and max time from admission to completion. */
 int vqc_serve_timing(vqc_server s, double* out);
+/* out[0..3]: over the loop iterations that launched work, the summed host time
+ * building and enqueueing the batched launches, the summed wait for the device,
+ * the summed host time retiring finished requests (seconds), and the number of
+ * such iterations.  Diagnostic; the reference has no serving loop. */
+int vqc_serve_loop_timing(vqc_server s, double* out);
 int vqc_serve_close(vqc_server s);
 
 #ifdef __cplusplus

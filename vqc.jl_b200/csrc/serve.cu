@@ -111,6 +111,10 @@ struct vqc_server_s {
   // statistics
   long long completed = 0, iterations = 0, launches = 0, items_launched = 0;
   double plan_s_max = 0, wait_s_max = 0, run_s_max = 0, plan_s_sum = 0, wait_s_sum = 0, run_s_sum = 0;
+  // loop iterations with work: host time building and enqueueing, time waiting for the
+  // device, host time retiring (seconds, summed)
+  double loop_build_s = 0, loop_wait_s = 0, loop_retire_s = 0;
+  long long loop_busy = 0;
   std::string fatal;
 };
 
@@ -281,6 +285,7 @@ static void worker_main(vqc_server_s* s) {
       s->active.push_back(r);
     }
     // 2. one launch per step kind (and tile size) over every active request
+    const double t_build = now_s();
     std::vector<TileItem> fwd_items[13], adj_items[13];
     std::vector<RedItem> red_items;
     std::vector<PauliItem> p_items[2];  // [0] energy only, [1] energy + cotangent
@@ -476,7 +481,9 @@ static void worker_main(vqc_server_s* s) {
                                  cudaMemcpyDeviceToHost, s->stream));
       }
     SRV_CK(cudaEventRecord(s->ev, s->stream));
+    const double t_enqueued = now_s();
     SRV_CK(cudaEventSynchronize(s->ev));
+    const double t_synced = now_s();
     // 3. retire
     std::vector<std::shared_ptr<Request>> still;
     for (auto& r : s->active) {
@@ -508,6 +515,12 @@ static void worker_main(vqc_server_s* s) {
     }
     std::lock_guard<std::mutex> lk(s->mu);
     s->active.swap(still);
+    if (nl > 0) {
+      s->loop_build_s += t_enqueued - t_build;
+      s->loop_wait_s += t_synced - t_enqueued;
+      s->loop_retire_s += now_s() - t_synced;
+      ++s->loop_busy;
+    }
     ++s->iterations;
     s->launches += nl;
     s->items_launched += ni;
@@ -655,6 +668,16 @@ int vqc_serve_timing(vqc_server s, double* out) {
   out[3] = s->wait_s_max;
   out[4] = s->run_s_sum / n;
   out[5] = s->run_s_max;
+  return VQC_OK;
+}
+
+int vqc_serve_loop_timing(vqc_server s, double* out) {
+  if (!s || !out) return fail(VQC_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  out[0] = s->loop_build_s;
+  out[1] = s->loop_wait_s;
+  out[2] = s->loop_retire_s;
+  out[3] = (double)s->loop_busy;
   return VQC_OK;
 }
 

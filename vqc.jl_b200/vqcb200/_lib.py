@@ -99,6 +99,7 @@ SIGNATURES = {
     "vqc_serve_wait": ([_H, ctypes.c_int64, _I, _D, _D], _I),
     "vqc_serve_stats": ([_H, ctypes.POINTER(ctypes.c_longlong)], _I),
     "vqc_serve_timing": ([_H, _D], _I),
+    "vqc_serve_loop_timing": ([_H, _D], _I),
     "vqc_serve_close": ([_H], _I),
 }
 

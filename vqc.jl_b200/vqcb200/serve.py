@@ -98,6 +98,15 @@ class Server:
         keys = ["plan_mean_s", "plan_max_s", "wait_mean_s", "wait_max_s", "run_mean_s", "run_max_s"]
         return dict(zip(keys, list(out)))
 
+    def loop_timing(self):
+        """Per busy loop iteration (one that launched work): mean host time building and
+        enqueueing, mean wait for the device, mean host time retiring (seconds)."""
+        out = (ctypes.c_double * 4)()
+        _lib.check(self._lib.vqc_serve_loop_timing(self._h, out))
+        n = max(out[3], 1.0)
+        return {"iterations": int(out[3]), "build_s": out[0] / n, "device_wait_s": out[1] / n,
+                "retire_s": out[2] / n}
+
     def close(self):
         if self._h:
             self._lib.vqc_serve_close(self._h)
