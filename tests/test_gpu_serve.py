@@ -35,9 +35,13 @@ def test_serve_matches_single_path_and_oracle():
         tickets = [srv.submit(n, W.to_circuit(spec), W.to_operator(h), want_grad=g) for n, spec, h, g in reqs]
         results = [srv.wait(t) for t in tickets]
         st = srv.stats()
+        lt = srv.loop_timing()
     assert st["completed"] == len(reqs)
     # batching happened: fewer launches than request-steps
     assert st["launches"] < st["request_steps"]
+    # every iteration that launched work is timed, in non-negative phases
+    assert 0 < lt["iterations"] <= st["iterations"]
+    assert min(lt["build_s"], lt["device_wait_s"], lt["retire_s"]) >= 0
     for (n, spec, hspec, g), (e, grads, lat) in zip(reqs, results):
         e_ref, g_ref = O.energy_and_gradient(O.from_spec(spec), O.terms_from_spec(hspec), O.zero_state(n), nthreads=4)
         assert abs(e - e_ref) / max(abs(e_ref), 1.0) < 1e-5
