@@ -5,7 +5,7 @@ Tolerances (stated once, used everywhere):
     normalised states and relative on scalars / gradient vectors;
   * FP32 (complex64) states with FP64 accumulation: 1e-5 relative on
     expectations (relative to max(|E|, 1): these Hamiltonians have norm of
-    order n, so an energy that cancels to ~0 is judged against that scale)
+    order n, so an energy that cancels to ~0 is compared against that scale)
     and norm-wise on gradients; 1e-5 max-abs on normalised states
     after short circuits (the error grows with circuit depth: long-circuit
     tests state their own bound).
