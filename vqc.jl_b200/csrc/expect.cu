@@ -128,6 +128,11 @@ __device__ __forceinline__ void pauli4_add(V (&hv)[4], const V (&W)[4], const V 
 #pragma unroll
   for (int a = 0; a < 4; ++a) hv[a] = cfma(W[a ^ AX], kv[a ^ AX], hv[a]);
 }
+template <int AX, class V>
+__device__ __forceinline__ void pauli4_add1(V (&hv)[4], const V& f, const V (&kv)[4]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) hv[a] = cfma(f, kv[a ^ AX], hv[a]);
+}
 template <class V>
 __device__ __forceinline__ void pauli4_wh(const V (&F)[4], V (&W)[4]) {
   V s01, d01, s23, d23;
@@ -178,6 +183,30 @@ __global__ void __launch_bounds__(kRedThreads)
       const int64_t jb = i0 ^ (int64_t)(g.x & ~3ull);
       V kv[4];
       load4<R>(ket + jb, kv);
+      if (g.cs[1] == g.cs[4]) {
+        // every term of the group in class 0 (no Z on the two lowest qubits): the
+        // same phase at all four partners, W[b] = F[0] (uniform over the grid)
+        V f = zero, fd = zero;
+        for (int q = g.cs[0]; q < g.cs[1]; ++q) {
+          const uint64_t m = (uint64_t)jb & st[q].z;
+          const bool odd = (__popc((unsigned)m ^ (unsigned)(m >> 32)) & 1) != 0;
+          const V cc = st[q].c;
+          f.x += odd ? -cc.x : cc.x;
+          f.y += odd ? -cc.y : cc.y;
+          if (SEP) {
+            const V dd = st[q].d;
+            fd.x += odd ? -dd.x : dd.x;
+            fd.y += odd ? -dd.y : dd.y;
+          }
+        }
+        switch ((int)(g.x & 3)) {  // (compile-time register indices)
+          case 0: pauli4_add1<0>(hv, f, kv); if (SEP) pauli4_add1<0>(ov, fd, kv); break;
+          case 1: pauli4_add1<1>(hv, f, kv); if (SEP) pauli4_add1<1>(ov, fd, kv); break;
+          case 2: pauli4_add1<2>(hv, f, kv); if (SEP) pauli4_add1<2>(ov, fd, kv); break;
+          default: pauli4_add1<3>(hv, f, kv); if (SEP) pauli4_add1<3>(ov, fd, kv); break;
+        }
+        continue;
+      }
       V F[4], Fd[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
