@@ -2,12 +2,14 @@
 matrices (applygates/apply_qmaps.jl, hamiltonian/expecs_dm/expecs_dm.jl)
 against the oracle's restatement, and the oracle against dense NumPy
 (rho -> sum_i K_i rho K_i^dagger; tr(H rho)).
-Tolerances: helpers.tol (1e-12 FP64, 1e-5 FP32), scaled by the depth."""
+Bounds: helpers.py (1e-12 FP64, 1e-5 FP32), asserted as stated against the
+oracle run on the same FP32-rounded input; density matrices after channels
+and cotangent matrices (not normalised) are compared norm-wise."""
 import numpy as np
 import pytest
 
 import vqcb200 as V
-from helpers import max_abs, rand_psi, tol
+from helpers import as_input, max_abs, max_rel, rand_psi, rel, rel_scalar, tol
 from oracle import dense_np as D
 from oracle import gates_ref as GR
 from oracle import oracle as O
@@ -38,25 +40,25 @@ def test_channels_on_density_matrix(dtype):
     n = 6
     psi = rand_psi(rng, n)
     rho = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
-    ref = O.density_matrix(psi)
+    ref = O.density_matrix(as_input(psi, dtype))
     maps = [V.Depolarizing(1, 0.1), V.AmplitudeDamping(4, 0.3), V.PhaseDamping(6, 0.25),
             V.QuantumMap((2, 5), _kraus2(rng)), V.QuantumMap((6, 1), _kraus2(rng))]
     for m in maps:
         V.apply(m, rho)
         O.dm_apply_channel(ref, n, [p - 1 for p in m.positions], m.kraus)
-    assert max_abs(rho.data(), ref) < tol(dtype) * 10
-    assert abs(rho.tr() - 1) < tol(dtype) * 10  # trace preserving
+    assert max_abs(rho.data(), ref) < tol(dtype)
+    assert abs(rho.tr() - 1) < tol(dtype)  # trace preserving
     # adjoint and inverse of the supermatrix
     m = V.QuantumMap((3, 2), _kraus2(rng))
     V.apply_dagger(m, rho)
     O.dm_apply_channel(ref, n, [2, 1], m.kraus, mode=1)
-    assert max_abs(rho.data(), ref) < tol(dtype) * 10
+    assert max_rel(rho.data(), ref) < tol(dtype)
     m = V.AmplitudeDamping(3, 0.2)
     V.apply(m, rho)
     V.apply_inverse(m, rho)
     O.dm_apply_channel(ref, n, [2], m.kraus, mode=0)
     O.dm_apply_channel(ref, n, [2], m.kraus, mode=2)
-    assert max_abs(rho.data(), ref) < tol(dtype) * 10
+    assert max_rel(rho.data(), ref) < tol(dtype)
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
@@ -75,14 +77,14 @@ def test_noisy_circuit_on_state(dtype):
     psi = rand_psi(rng, n)
     out = V.apply(c, V.StateVector(psi.astype(dtype), dtype=dtype))
     assert isinstance(out, V.DensityMatrix)
-    ref = O.density_matrix(psi)
+    ref = O.density_matrix(as_input(psi, dtype))
     for g in c:
         pos = [p - 1 for p in g.positions]
         if isinstance(g, V.QuantumMap):
             O.dm_apply_channel(ref, n, pos, g.kraus)
         else:
             O.dm_apply_gate(ref, n, pos, g.mat)
-    assert max_abs(out.data(), ref) < tol(dtype) * 10
+    assert max_abs(out.data(), ref) < tol(dtype)
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
@@ -92,18 +94,18 @@ def test_dm_pauli_expectation(dtype, n):
     psi = rand_psi(rng, n)
     rho = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
     V.apply(V.Depolarizing(1, 0.2), rho)
-    ref = O.dm_apply_channel(O.density_matrix(psi), n, [0], V.Depolarizing(1, 0.2).kraus)
+    ref = O.dm_apply_channel(O.density_matrix(as_input(psi, dtype)), n, [0], V.Depolarizing(1, 0.2).kraus)
     spec = [({1: "X", n: "Y"}, 0.36), ({1: "Z", 2: "Z"}, -0.8), ({2: "Y"}, 0.5 + 0.25j), ({n: "X", 1: "Z"}, 1.3),
             ({}, 0.1)]
     H = V.QubitsOperator(*[V.QubitsTerm(ops, coeff=c) for ops, c in spec])
     terms = [O.make_term({q - 1: o for q, o in ops.items()}, c) for ops, c in spec]
     got = V.expectation(H, rho)
     want = O.dm_expectation(terms, ref, n)
-    assert abs(got - want) < tol(dtype) * 10 * max(1.0, abs(want))
+    assert rel_scalar(got, want) < tol(dtype)
     # a pure state: tr(H |psi><psi|) = <psi|H|psi>
     pure = V.DensityMatrix(V.StateVector(psi.astype(dtype), dtype=dtype))
     sv = V.expectation(H, V.StateVector(psi.astype(dtype), dtype=dtype))
-    assert abs(V.expectation(H, pure) - sv) < tol(dtype) * 10 * max(1.0, abs(sv))
+    assert rel_scalar(V.expectation(H, pure), sv) < tol(dtype)
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
@@ -145,13 +147,12 @@ def test_noisy_dm_gradient(dtype, loss):
             rho_ref = O.dm_apply_channel(rho_ref, n, it[1], it[2])
         else:
             O.dm_apply_gate(rho_ref, n, it[1], it[2])
-    assert max_abs(rho.data(), rho_ref) < tol(dtype) * 10
-    g_ref, d_ref, y_ref = O.dm_circuit_gradient(ref_items, rho_ref, dmat.reshape(-1, order="F").copy(), n)
+    assert max_abs(rho.data(), rho_ref) < tol(dtype)
+    g_ref, d_ref, y_ref = O.dm_circuit_gradient(ref_items, rho_ref, as_input(dmat.reshape(-1, order="F"), dtype), n)
     d, g, y = V.back_propagate(delta, c, rho)
-    scale = max(1.0, np.abs(g_ref).max())
-    assert np.abs(g - g_ref).max() < (1e-10 if dtype == np.complex128 else 5e-5) * scale
-    assert max_abs(y.data(), y_ref) < tol(dtype) * 100
-    assert max_abs(d.data(), d_ref) < tol(dtype) * 100 * max(1.0, np.abs(d_ref).max())
+    assert rel(g, g_ref) < tol(dtype)
+    assert max_rel(y.data(), y_ref) < tol(dtype)
+    assert rel(d.data(), d_ref) < tol(dtype)
 
 
 def _golden_noisy_items(d):
@@ -190,18 +191,17 @@ def test_golden_noisy_dm(dtype):
     rho = V.DensityMatrix(V.StateVector(d["psi"].astype(dtype), dtype=dtype))
     c = V.QCircuit(items)
     V.apply(c, rho)
-    assert max_abs(rho.data(), d["rho"]) < tol(dtype) * 10
+    assert max_abs(rho.data(), d["rho"]) < tol(dtype)
     H = V.QubitsOperator(*[V.QubitsTerm({q + 1: "IXZY"[((int(x) >> q) & 1) | (((int(z) >> q) & 1) << 1)]
                                           for q in range(n) if ((int(x) | int(z)) >> q) & 1}, coeff=complex(cf))
                             for x, z, cf in zip(d["xmask"], d["zmask"], d["coeff"])])
     e = V.expectation(H, rho)
-    assert abs(e - d["energy"]) < tol(dtype) * 10
+    assert rel_scalar(e, d["energy"]) < tol(dtype)
     terms = [O.make_term({q: "IXZY"[((int(x) >> q) & 1) | (((int(z) >> q) & 1) << 1)]
                           for q in range(n) if ((int(x) | int(z)) >> q) & 1}, complex(cf))
              for x, z, cf in zip(d["xmask"], d["zmask"], d["coeff"])]
     dmat = D.pauli_sum_matrix(n, terms).conj().T
     delta = V.DensityMatrix(dmat.astype(dtype), dtype=dtype)
     dd, g, _ = V.back_propagate(delta, c, rho)
-    scale = max(1.0, np.abs(d["grads"]).max())
-    assert np.abs(g - d["grads"]).max() < (1e-10 if dtype == np.complex128 else 5e-5) * scale
-    assert max_abs(dd.data(), d["delta_in"]) < tol(dtype) * 100 * max(1.0, np.abs(d["delta_in"]).max())
+    assert rel(g, d["grads"]) < tol(dtype)
+    assert rel(dd.data(), d["delta_in"]) < tol(dtype)
