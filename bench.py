@@ -164,6 +164,24 @@ def cpu_sample(nthreads, reps=1, n=N_QUBITS, dtype=np.complex64):
     return 1.0 / per_grad, sample_s
 
 
+def cpu_full_check(nthreads, n=20):
+    """The extrapolation behind cpu_sample checked against one timed full
+    gradient of the same workload at a smaller size (n qubits, all 20 layers,
+    FP32): returns the measured and extrapolated seconds per gradient."""
+    from oracle import oracle as O
+    from vqcb200 import workloads as W
+    rng = np.random.default_rng(SEED)
+    theta = rng.uniform(0, 2 * np.pi, LAYERS * (4 * n - 1))
+    gates = O.from_spec(W.rxyz_crx_spec(n, LAYERS, theta))
+    terms = O.terms_from_spec(W.xxz_spec(n, 0.5))
+    t0 = time.perf_counter()
+    O.energy_and_gradient(gates, terms, O.zero_state(n, np.complex64), nthreads=nthreads)
+    measured = time.perf_counter() - t0
+    rate, _ = cpu_sample(nthreads, reps=8, n=n)
+    return {"n_qubits": n, "measured_s_per_gradient": measured, "extrapolated_s_per_gradient": 1.0 / rate,
+            "measured_over_extrapolated": measured * rate}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -250,7 +268,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         prof = None
         if profile:
-            prof = _lib.profile_read()
+            prof = _lib.profile_read(with_flops=True)
             _lib.profile_enable(False)
         ms = start.elapsed_time(end) / steps
         if world > 1:
@@ -281,32 +299,50 @@ def run_ours(args, rank, world, local_rank):
     fp64 = None
     if not args.no_fp64:
         psi64 = make_state(np.complex128)
-        ms64, _, energy64, grads64 = timed(psi64, max(1, args.steps // 2), 1)
+        ms64, prof64, energy64, grads64 = timed(psi64, max(1, args.steps // 2), 1, profile=True)
         del psi64
         fp64 = {"value": world * 1000.0 / ms64, "unit": UNIT, "ms_per_step": ms64, "fp32_speedup": ms64 / ms,
                 "energy_rel_diff_fp32_vs_fp64": abs(energy - energy64) / abs(energy64),
                 "grad_rel_diff_fp32_vs_fp64": float(np.linalg.norm(grads - grads64) / np.linalg.norm(grads64))}
 
+    # measured FMA-pipe peaks: the compute roofline of the tile passes
+    fma32 = _lib.fma_peak(local_rank, 0)
+    fma64 = _lib.fma_peak(local_rank, 2)
+
     if rank != 0:
         return
     hbm, peak_kind = peaks()
+    if fp64 is not None:
+        fp64["kernels"] = kernel_rooflines(prof64, max(1, args.steps // 2), ms64, hbm, fma64)
+        fp64["fma_peak_tflops_fp64"] = fma64
     dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None  # largest total device time
     roof = None
     launches = sum(v[0] for k, v in prof.items() if not k.startswith("plan_")) if prof else 0
     if dom:
-        name, (n, tot_ms, tot_bytes) = dom
+        name, (n, tot_ms, tot_bytes, tot_flops) = dom
         achieved = tot_bytes / (tot_ms * 1e-3) / 1e9
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                 "bytes_per_launch": tot_bytes / n, "avg_launch_ms": tot_ms / n,
-                "share_of_step": tot_ms / (ms * args.steps), "traffic": traffic_from_profiles(name)}
+                "share_of_step": tot_ms / (ms * args.steps), "traffic": traffic_from_profiles(name),
+                "compute": {"pipe": "FP32 FMA (packed fma.rn.f32x2)", "unit": "TFLOP/s",
+                            "achieved": tot_flops / (tot_ms * 1e-3) / 1e12, "peak": fma32,
+                            "frac": tot_flops / (tot_ms * 1e-3) / 1e12 / fma32 if fma32 else None,
+                            "flops_per_launch": tot_flops / n,
+                            "peak_kind": "measured on this GPU by vqc_fma_peak (calibration kernel)"}}
     cpu = None
     if world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
         v, s = cpu_sample(nthreads, reps=8)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
                "sample": "8 x (2 rotations + 1 CRX forward/reverse sweep) + one XXZ key at n=26, FP32, scaled "
-                         "to one gradient (%.1f s of CPU work)" % s}
+                         "to one gradient (%.1f s of CPU work)" % s,
+               "extrapolation_check": cpu_full_check(nthreads)}
+    secondary = None
+    if world == 1 and not args.no_secondary:
+        secondary = {"gates_n30": gates_record(30, 3, local_rank), "dm_n13": dm_record(13, local_rank),
+                     "serve": serve_record(local_rank, requests=2000, rates=[1000.0], baseline_requests=100,
+                                           memory_mib=args.serve_memory, slots=args.serve_slots)}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded angles, |0> input)",
@@ -316,8 +352,8 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": packed.nparams * 8 + 16},
             "fp64_plain": fp64,
             "energy": energy.real,
-            "roofline": roof, "kernels": {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in (prof or {}).items()},
-            "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu}
+            "roofline": roof, "kernels": kernel_rooflines(prof, args.steps, ms, hbm, fma32),
+            "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu, "secondary": secondary}
     print(json.dumps(line), flush=True)
 
 
@@ -327,9 +363,32 @@ def _events(stream):
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def run_gates_n30(args, local_rank):
-    """30 qubits: per-gate-class HBM GB/s of single gates, and the fused-block
-    speedup of 10 layers of (U3 on every qubit, CZ brickwork, one Toffoli)."""
+def kernel_rooflines(prof, steps, ms_step, hbm, fma):
+    """Per kernel class of the profile: launches, device time, algorithmic
+    bytes, and for each class its HBM fraction (algorithmic bytes / time over
+    the measured HBM peak) and, where it counts FMA-pipe flops, its fraction
+    of the measured FMA peak `fma` (TFLOP/s)."""
+    out = {}
+    for k, v in (prof or {}).items():
+        n, tms, tby = v[0], v[1], v[2]
+        fl = v[3] if len(v) > 3 else 0.0
+        rec = {"launches": n, "ms": tms, "bytes": tby}
+        if tms > 0 and tby > 0:
+            gbs = tby / (tms * 1e-3) / 1e9
+            rec.update({"avg_launch_ms": tms / n, "GB/s": gbs, "frac_of_hbm": gbs / hbm,
+                        "share_of_step": tms / (ms_step * steps)})
+        if tms > 0 and fl > 0:
+            tf = fl / (tms * 1e-3) / 1e12
+            rec.update({"fma_pipe_TFLOP/s": tf, "frac_of_fma_peak": tf / fma if fma else None})
+        out[k] = rec
+    return out
+
+
+def gates_record(n, steps, local_rank):
+    """n qubits (30: 16 GiB in FP64, 8 GiB in FP32): per-gate-class HBM GB/s of
+    single gates (algorithmic bytes over event time, fraction of the measured
+    HBM peak), and the fused-block speedup of 10 layers of (U3 on every qubit,
+    CZ brickwork, one Toffoli)."""
     import torch
     import vqcb200 as V
     from vqcb200 import _lib
@@ -337,8 +396,7 @@ def run_gates_n30(args, local_rank):
     torch.cuda.set_device(local_rank)
     lib = V.load()
     hbm, peak_kind = peaks()
-    n = args.qubits or 30
-    out = {"metric": "HBM GB/s per gate class and fused-block speedup, n=%d" % n, "unit": "GB/s", "n_gpus": 1,
+    out = {"metric": "HBM GB/s per gate class and fused-block speedup, n=%d" % n, "unit": "GB/s",
            "config": {"workload": "10 x (U3 on every qubit, CZ brickwork, 1 Toffoli), n=%d" % n}, "classes": {}}
     spec = W.u3_cz_toffoli_spec(n, 10, SEED)
     circuit = W.to_circuit(spec)
@@ -356,7 +414,7 @@ def run_gates_n30(args, local_rank):
                 V.apply(g, psi)
             _lib.profile_enable(True)
             a, b = _events(stream)
-            reps = max(1, args.steps)
+            reps = max(1, steps)
             a.record(stream)
             for _ in range(reps):
                 V.apply(g, psi)
@@ -388,19 +446,19 @@ def run_gates_n30(args, local_rank):
         out["classes"][name] = res
         del psi
     out["peak"] = {"hbm_GB/s": hbm, "kind": peak_kind}
-    print(json.dumps(out), flush=True)
+    return out
 
 
-def run_dm_n13(args, local_rank):
-    """Density matrix, 13 qubits (1 GiB complex128): seeded random pure state,
-    8 layers of U3 on every qubit + CNOT ladder as rho <- U rho U^dagger,
-    partial trace over the top 4 qubits, basis probabilities."""
+def dm_record(n, local_rank):
+    """Density matrix of n qubits (13: 1 GiB complex128): seeded random pure
+    state, 8 layers of U3 on every qubit + CNOT ladder as rho <- U rho
+    U^dagger, partial trace over the top 4 qubits, basis probabilities."""
     import torch
     import vqcb200 as V
     from vqcb200 import workloads as W
     torch.cuda.set_device(local_rank)
     lib = V.load()
-    n = args.qubits or 13
+    hbm, _ = peaks()
     rng = np.random.default_rng(SEED)
     psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
     psi /= np.linalg.norm(psi)
@@ -426,24 +484,26 @@ def run_dm_n13(args, local_rank):
     probs = V.probabilities(rho)
     t_probs = time.perf_counter() - t0
     S = (1 << (2 * n)) * 16
-    out = {"metric": "density-matrix circuit time, n=%d (rho %d MiB)" % (n, S >> 20), "unit": "ms",
-           "config": {"workload": "8 x (U3 on every qubit + CNOT ladder) on rho, ptrace of the top 4 qubits, "
-                                  "probabilities", "gates": len(circuit)},
-           "circuit_ms_one_by_one": res["unfused"], "circuit_ms_fused": res["fused"],
-           "fused_speedup": res["unfused"] / res["fused"],
-           "one_by_one_GB/s_per_gate": len(circuit) * 2 * S / (res["unfused"] * 1e-3) / 1e9,
-           "ptrace_ms_host_call": t_ptrace * 1e3, "probs_ms_host_call": t_probs * 1e3,
-           "trace_of_reduced": float(np.trace(red).real), "sum_probs": float(probs.sum())}
-    print(json.dumps(out), flush=True)
+    per_gate = len(circuit) * 2 * S / (res["unfused"] * 1e-3) / 1e9
+    return {"metric": "density-matrix circuit time, n=%d (rho %d MiB)" % (n, S >> 20), "unit": "ms",
+            "config": {"workload": "8 x (U3 on every qubit + CNOT ladder) on rho, ptrace of the top 4 qubits, "
+                                   "probabilities", "gates": len(circuit)},
+            "circuit_ms_one_by_one": res["unfused"], "circuit_ms_fused": res["fused"],
+            "fused_speedup": res["unfused"] / res["fused"],
+            "one_by_one_GB/s_per_gate": per_gate, "one_by_one_frac_of_hbm": per_gate / hbm,
+            "ptrace_ms_host_call": t_ptrace * 1e3, "probs_ms_host_call": t_probs * 1e3,
+            "trace_of_reduced": float(np.trace(red).real), "sum_probs": float(probs.sum())}
 
 
-def run_serve(args, local_rank):
+def serve_record(local_rank, requests=2000, rates=(500.0, 1000.0, 2000.0, 4000.0), baseline_requests=200,
+                 memory_mib=16384, slots=512):
     """Serving stream (continuous batching): requests with n ~ U{10..22},
     depth ~ U{2..12} layers of the hardware-efficient ansatz (RY, RZ on every
     qubit + CNOT ladder), angles ~ U[0, 2 pi), half energy only and half energy
     + gradient, transverse-field Ising H with g ~ U[0.2, 1.5]; Poisson arrivals
-    at swept rates.  FP32 states, FP64 accumulation.  Baseline: one request at
-    a time through the plain FP64 single-request path, same arrival sequence."""
+    at each offered rate.  FP32 states, FP64 accumulation.  Baseline: one
+    request at a time through the plain FP64 single-request path, same arrival
+    sequence."""
     import threading
 
     import torch
@@ -454,7 +514,7 @@ def run_serve(args, local_rank):
     torch.cuda.set_device(local_rank)
     V.load()
     rng = np.random.default_rng(SEED)
-    nreq = args.requests
+    nreq = requests
     reqs = []
     for i in range(nreq):
         n = int(rng.integers(10, 23))
@@ -471,8 +531,8 @@ def run_serve(args, local_rank):
         """Submit `count` requests with Poisson arrivals at `rate`/s; latencies in s."""
         arrivals = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, count))
         lat = [None] * count
-        with Server(device=local_rank, dtype=np.complex64, memory_bytes=args.serve_memory << 20,
-                    max_active=args.serve_slots, planner_threads=4) as srv:
+        with Server(device=local_rank, dtype=np.complex64, memory_bytes=memory_mib << 20,
+                    max_active=slots, planner_threads=4) as srv:
             tickets = [None] * count
             done = threading.Event()
 
@@ -529,17 +589,16 @@ def run_serve(args, local_rank):
 
     # warm-up (kernel loads, allocator pools)
     stream(200.0, min(200, nreq))
-    rates = [float(r) for r in args.rates.split(",")]
-    results = [stream(r, nreq) for r in rates]
+    results = [stream(float(r), nreq) for r in rates]
     # service rate of the one-at-a-time baseline: back-to-back requests
-    base_sat = baseline(1e6, min(args.baseline_requests, nreq))
-    base = [baseline(r, min(args.baseline_requests, nreq)) for r in rates if r < 0.9 * base_sat["throughput"]]
-    out = {"metric": "serving throughput and p50/p99 latency (continuous batching, FP32 states)", "unit": "requests/s",
-           "config": {"workload": "n~U{10..22}, 2..12 HEA layers, 50% energy / 50% energy+gradient, TFIM g~U[0.2,1.5], "
-                                  "Poisson arrivals", "requests_per_rate": nreq, "memory_budget_MiB": args.serve_memory,
-                      "slots": args.serve_slots},
-           "served": results, "baseline_fp64_one_at_a_time": {"saturated": base_sat, "at_rates": base}}
-    print(json.dumps(out), flush=True)
+    base_sat = baseline(1e6, min(baseline_requests, nreq))
+    base = [baseline(float(r), min(baseline_requests, nreq)) for r in rates if r < 0.9 * base_sat["throughput"]]
+    return {"metric": "serving throughput and p50/p99 latency (continuous batching, FP32 states)",
+            "unit": "requests/s",
+            "config": {"workload": "n~U{10..22}, 2..12 HEA layers, 50% energy / 50% energy+gradient, TFIM "
+                                   "g~U[0.2,1.5], Poisson arrivals", "requests_per_rate": nreq,
+                       "memory_budget_MiB": memory_mib, "slots": slots},
+            "served": results, "baseline_fp64_one_at_a_time": {"saturated": base_sat, "at_rates": base}}
 
 
 def main():
@@ -551,12 +610,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the secondary records (gate classes at n=30, density matrix n=13, serving)")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests per rate")
     ap.add_argument("--rates", default="500,1000,2000,4000", help="serve: offered rates (requests/s)")
     ap.add_argument("--baseline-requests", type=int, default=200, help="serve: requests of the FP64 baseline")
     ap.add_argument("--serve-memory", type=int, default=16384, help="serve: device memory budget (MiB)")
     ap.add_argument("--serve-slots", type=int, default=512, help="serve: requests in flight at most")
-    ap.add_argument("--workload", default="adjoint", choices=["adjoint", "gates_n30", "dm_n13", "serve"],
+    ap.add_argument("--workload", default="adjoint", choices=["adjoint", "gates_n30", "dm_n13", "serve", "fma_peak"],
                     help="adjoint (the headline) or a secondary workload")
     ap.add_argument("--qubits", type=int, default=None,
                     help="state size (default 26, the headline; smaller sizes are for profiling captures)")
@@ -571,13 +632,22 @@ def main():
         run_reference(args, rank, world)
         return
     if args.workload == "gates_n30":
-        run_gates_n30(args, local_rank)
+        print(json.dumps(gates_record(args.qubits or 30, args.steps, local_rank)), flush=True)
         return
     if args.workload == "dm_n13":
-        run_dm_n13(args, local_rank)
+        print(json.dumps(dm_record(args.qubits or 13, local_rank)), flush=True)
         return
     if args.workload == "serve":
-        run_serve(args, local_rank)
+        print(json.dumps(serve_record(local_rank, args.requests, [float(r) for r in args.rates.split(",")],
+                                      args.baseline_requests, args.serve_memory, args.serve_slots)), flush=True)
+        return
+    if args.workload == "fma_peak":
+        import vqcb200 as V
+        from vqcb200 import _lib
+        V.load()
+        print(json.dumps({"metric": "measured FMA-pipe peak", "unit": "TFLOP/s",
+                          "fp32_packed": _lib.fma_peak(local_rank, 0), "fp32_scalar": _lib.fma_peak(local_rank, 1),
+                          "fp64": _lib.fma_peak(local_rank, 2)}), flush=True)
         return
     if world > 1:
         import torch

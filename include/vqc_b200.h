@@ -43,6 +43,7 @@ extern "C" {
 #define VQC_ERR_UNSUPPORTED (-4) /* e.g. a >5-qubit gate (generic.jl:37) */
 #define VQC_ERR_TIMEOUT (-5)     /* a bounded wait ran out (serving) */
 #define VQC_ERR_BUSY (-6)        /* serving: no slot or memory free for the request now */
+#define VQC_ERR_CANCELED (-7)    /* serving: the request was cancelled */
 
 #define VQC_C64 0  /* ComplexF32 amplitudes */
 #define VQC_C128 1 /* ComplexF64 amplitudes */
@@ -124,6 +125,16 @@ void* vqc_state_stream(vqc_state h);
 int vqc_profile_enable(int on);
 int vqc_profile_count(void);
 int vqc_profile_get(int i, char* name, int name_len, long long* launches, double* total_ms, double* total_bytes);
+/* Total FMA-pipe flops of record i: 2 x the lane operations of the FMA pipe
+ * (fused multiply-adds, multiplies, adds) the class's launches execute, for
+ * the kernels bound by arithmetic (the tile passes); 0 for the others. */
+int vqc_profile_flops(int i, double* total_flops);
+/* Measured peak of the device's FMA pipe in TFLOP/s (2 flops per FMA lane):
+ * a calibration kernel of independent FMA chains on every SM, timed with
+ * CUDA events.  kind 0: packed two-lane FP32 (fma.rn.f32x2), 1: scalar
+ * FP32, 2: FP64.  The compute roofline of the tile passes (no counterpart
+ * in the reference). */
+int vqc_fma_peak(int device, int kind, double* tflops);
 
 /* ---- gates: apply!(::Gate, ::StateVector) (applygates/generic/generic.jl:6-14,
  *      _apply_gate_threaded2! in threaded_short_range.jl / threaded_long_range.jl,
@@ -235,8 +246,11 @@ typedef struct vqc_server_s* vqc_server;
 int vqc_serve_open(int device, int dtype, size_t memory_bytes, int max_active, int planner_threads,
                    vqc_server* out);
 /* Queues one request (inputs are copied).  grads_out (nparams doubles) must
- * stay valid until the request is finished.  Gates must have at most two
- * target qubits (controls read off the matrix), 9..40 qubits. */
+ * stay valid until vqc_serve_poll / vqc_serve_wait has reported the request's
+ * outcome (a result, an error, or VQC_ERR_CANCELED).  Gates must have at
+ * most two target qubits (controls read off the matrix), 9..40 qubits.  A
+ * request with a non-finite matrix entry or Pauli coefficient is rejected
+ * here (VQC_ERR_ARG) and never reaches the device. */
 int vqc_serve_submit(vqc_server s, int nqubits, const vqc_gate* gates, int ngates, const double* mats,
                      const vqc_param* params, int nparams, const vqc_pauli* terms, int nterms, int want_grad,
                      double* grads_out, int64_t* ticket);
@@ -245,6 +259,14 @@ int vqc_serve_submit(vqc_server s, int nqubits, const vqc_gate* gates, int ngate
 int vqc_serve_poll(vqc_server s, int64_t ticket, double* energy, double* latency_s);
 /* As vqc_serve_poll but waits up to timeout_ms (then VQC_ERR_TIMEOUT). */
 int vqc_serve_wait(vqc_server s, int64_t ticket, int timeout_ms, double* energy, double* latency_s);
+/* Cancels a request: one still queued or planned is dropped at once, one
+ * running is retired at the worker's next iteration (its device memory goes
+ * back to the budget, its partial results are discarded).  Returns 1 when the
+ * cancellation was registered before the request finished -- poll / wait then
+ * report VQC_ERR_CANCELED and release the ticket -- 0 when it had already
+ * finished (its result stays available), negative for an unknown ticket.
+ * Requests batched with it are not affected. */
+int vqc_serve_cancel(vqc_server s, int64_t ticket);
 /* out[0..6]: completed, loop iterations, launches, request-steps launched,
  * device bytes admitted, requests running, requests waiting. */
 int vqc_serve_stats(vqc_server s, long long* out);

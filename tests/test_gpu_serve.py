@@ -138,3 +138,80 @@ def test_wait_timeout():
         with pytest.raises(TimeoutError):
             srv.wait(t, timeout=0.0)
         srv.wait(t)
+
+
+def test_cancel_queued_and_running_requests():
+    """vqc_serve_cancel: a request still waiting for admission (one slot, the
+    slot taken) is dropped at once; a running one is retired at the next
+    iteration with its memory back in the budget; the others finish with the
+    same results as alone."""
+    from vqcb200._lib import Cancelled
+    rng = np.random.default_rng(56)
+    big = make_request(rng, 22, 12)
+    small = [make_request(rng, 10, 2) for _ in range(3)]
+    with Server(dtype=np.complex64, memory_bytes=1 << 30, max_active=1) as srv:
+        t_run = srv.submit(22, W.to_circuit(big[0]), W.to_operator(big[1]))
+        ts = [srv.submit(10, W.to_circuit(s), W.to_operator(h)) for s, h in small]
+        t_queued = ts[1]
+        assert srv.cancel(t_queued) is True
+        assert srv.cancel(t_run) is True
+        with pytest.raises(Cancelled):
+            srv.wait(t_run)
+        with pytest.raises(Cancelled):
+            srv.wait(t_queued)
+        for i in (0, 2):
+            e, g, _ = srv.wait(ts[i])
+            e_ref, g_ref = O.energy_and_gradient(O.from_spec(small[i][0]), O.terms_from_spec(small[i][1]),
+                                                 O.zero_state(10), nthreads=4)
+            assert abs(e - e_ref) / max(abs(e_ref), 1.0) < 1e-5
+            assert rel(g, g_ref) < 1e-5
+        # a finished request cannot be cancelled; its result is still collected
+        t_done = srv.submit(10, W.to_circuit(small[0][0]), W.to_operator(small[0][1]))
+        while srv.stats()["completed"] < 3:
+            time.sleep(0.01)
+        assert srv.cancel(t_done) is False
+        srv.wait(t_done)
+        st = srv.stats()
+    assert st["completed"] == 3 and st["bytes_admitted"] == 0
+
+
+def test_poisoned_request_is_rejected_and_isolated():
+    """A request carrying a NaN gate entry (or an infinite Pauli coefficient)
+    is refused at submission; requests submitted around it, batched together,
+    give the oracle's results."""
+    rng = np.random.default_rng(57)
+    reqs = [(int(n),) + make_request(rng, int(n), 3) for n in rng.integers(9, 15, 6)]
+    with Server(dtype=np.complex64, memory_bytes=1 << 30, max_active=16) as srv:
+        ts = [srv.submit(n, W.to_circuit(s), W.to_operator(h)) for n, s, h in reqs[:3]]
+        poisoned = V.QCircuit([V.RxGate(1, float("nan"), isparas=True), V.CNOTGate(1, 2)])
+        with pytest.raises(ValueError):
+            srv.submit(9, poisoned, V.QubitsOperator(V.pauli({1: "Z"})))
+        with pytest.raises(ValueError):
+            srv.submit(9, W.to_circuit(reqs[0][1][:4]),
+                       V.QubitsOperator(V.QubitsTerm({1: "Z"}, coeff=float("inf"))))
+        ts += [srv.submit(n, W.to_circuit(s), W.to_operator(h)) for n, s, h in reqs[3:]]
+        out = [srv.wait(t) for t in ts]
+    for (n, spec, hspec), (e, g, _) in zip(reqs, out):
+        e_ref, g_ref = O.energy_and_gradient(O.from_spec(spec), O.terms_from_spec(hspec), O.zero_state(n), nthreads=4)
+        assert abs(e - e_ref) / max(abs(e_ref), 1.0) < 1e-5
+        assert rel(g, g_ref) < 1e-5
+
+
+def test_slow_client_does_not_hold_the_server():
+    """A client that never collects its results: the loop still finishes every
+    request and returns its device memory to the budget; the results stay
+    available until collected (or the server closes)."""
+    rng = np.random.default_rng(58)
+    reqs = [make_request(rng, 12, 3) for _ in range(8)]
+    with Server(dtype=np.complex64, memory_bytes=64 << 20, max_active=2) as srv:
+        ts = [srv.submit(12, W.to_circuit(s), W.to_operator(h)) for s, h in reqs]
+        # collect only the last one; the others are left waiting for a client
+        srv.wait(ts[-1])
+        deadline = time.time() + 60
+        while srv.stats()["completed"] < len(reqs) and time.time() < deadline:
+            time.sleep(0.01)
+        st = srv.stats()
+        assert st["completed"] == len(reqs)
+        assert st["bytes_admitted"] == 0 and st["running"] == 0
+        e, g, _ = srv.wait(ts[0], timeout=0.0)  # finished long ago: no wait needed
+        assert np.isfinite(e.real) and g.shape == (36 * 2,)

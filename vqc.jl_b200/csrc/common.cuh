@@ -151,10 +151,13 @@ namespace vqc {
 // Per-kernel-class launch timing with CUDA events on the launching stream,
 // switched on by vqc_profile_enable(1).  Each record carries the launch's
 // algorithmic bytes (the data the operation must move at minimum), so
-// achieved bandwidth = bytes / time per class.
+// achieved bandwidth = bytes / time per class, and, where the kernel is bound
+// by arithmetic, its FMA-pipe operations (lane operations of the FMA pipe:
+// fused multiply-adds, multiplies and adds, counted once each) as flops =
+// 2 x operations, against the measured FMA peak (vqc_fma_peak).
 struct ProfScope {
   int token = -1;
-  ProfScope(cudaStream_t s, const char* cls, double bytes);
+  ProfScope(cudaStream_t s, const char* cls, double bytes, double flops = 0);
   ~ProfScope();
   cudaStream_t stream;
 };

@@ -21,6 +21,7 @@
 // are reduced in a fixed order).
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -77,6 +78,7 @@ struct Request {
   // progress
   int step = 0;
   int status = 0;  // 0 queued, 1 planned, 2 running, 3 done, < 0 error
+  bool cancel = false;  // set by vqc_serve_cancel; a running request is retired at the next iteration
   std::string error;
   double energy[2] = {0, 0};
   double t_submit = 0, t_planned = 0, t_admit = 0, t_done = 0;
@@ -189,7 +191,9 @@ static void planner_main(vqc_server_s* s) {
     }
     const int rc = plan_request(s, *r);
     std::lock_guard<std::mutex> lk(s->mu);
-    if (rc) {
+    if (r->status < 0) {
+      // cancelled while it was being planned
+    } else if (rc) {
       r->status = rc;
       r->error = vqc_last_error();
       r->t_done = now_s();
@@ -284,6 +288,34 @@ static void worker_main(vqc_server_s* s) {
       std::lock_guard<std::mutex> lk(s->mu);
       s->active.push_back(r);
     }
+    // cancelled requests leave before the launches are built (the previous
+    // iteration's launches have completed: the loop waited for them)
+    {
+      std::vector<std::shared_ptr<Request>> keep;
+      std::vector<std::shared_ptr<Request>> gone;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto& r : s->active) (r->cancel ? gone : keep).push_back(r);
+      }
+      for (auto& r : gone) {
+        SRV_CK(cudaFreeAsync(r->dmem, s->stream));
+        r->dmem = nullptr;
+        s->pinned_free.emplace(r->host_cap, r->host_res);
+        r->host_res = nullptr;
+      }
+      if (!gone.empty()) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto& r : gone) {
+          s->in_use -= r->dbytes;
+          r->status = VQC_ERR_CANCELED;
+          r->error = "request cancelled";
+          r->t_done = now_s();
+        }
+        s->active.swap(keep);
+        s->cv_done.notify_all();
+      }
+    }
+    if (s->active.empty()) continue;
     // 2. one launch per step kind (and tile size) over every active request
     const double t_build = now_s();
     std::vector<TileItem> fwd_items[13], adj_items[13];
@@ -497,8 +529,14 @@ static void worker_main(vqc_server_s* s) {
         r->dmem = nullptr;
         std::lock_guard<std::mutex> lk(s->mu);
         s->in_use -= r->dbytes;
-        r->status = 3;
         r->t_done = now_s();
+        if (r->cancel) {  // cancelled during its last step: the outcome is the cancellation
+          r->status = VQC_ERR_CANCELED;
+          r->error = "request cancelled";
+          s->cv_done.notify_all();
+          continue;
+        }
+        r->status = 3;
         ++s->completed;
         const double pl = r->t_planned - r->t_submit, wt = r->t_admit - r->t_planned, rn = r->t_done - r->t_admit;
         s->plan_s_sum += pl;
@@ -591,6 +629,13 @@ int vqc_serve_submit(vqc_server s, int nqubits, const vqc_gate* gates, int ngate
     if (params[j].gate < 0 || params[j].gate >= ngates || params[j].dmat < 0) return fail(VQC_ERR_ARG, "bad parameter");
     mlen = std::max(mlen, (size_t)params[j].dmat + ((size_t)2 << (2 * gates[params[j].gate].nq)));
   }
+  // a poisoned request (a NaN or infinite matrix entry or coefficient) is
+  // turned away here: it never reaches the device or the batch
+  for (size_t i = 0; i < mlen; ++i)
+    if (!std::isfinite(mats[i])) return fail(VQC_ERR_ARG, "request has a non-finite gate or derivative matrix entry");
+  for (int t = 0; t < nterms; ++t)
+    if (!std::isfinite(terms[t].coeff_re) || !std::isfinite(terms[t].coeff_im))
+      return fail(VQC_ERR_ARG, "request has a non-finite Pauli coefficient");
   r->mats.assign(mats, mats + mlen);
   if (r->grad) r->params.assign(params, params + nparams);
   r->terms.assign(terms, terms + nterms);
@@ -643,6 +688,28 @@ int vqc_serve_wait(vqc_server s, int64_t ticket, int timeout_ms, double* energy,
                                         [&] { return r->status < 0 || r->status == 3; });
   if (!done) return fail(VQC_ERR_TIMEOUT, "request not finished within the timeout");
   return finish_ticket(s, s->all.find(ticket), energy, latency_s);
+}
+
+int vqc_serve_cancel(vqc_server s, int64_t ticket) {
+  if (!s) return fail(VQC_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return fail(VQC_ERR_ARG, "unknown ticket");
+  auto r = it->second;
+  if (r->status == 3 || r->status < 0) return 0;
+  r->cancel = true;
+  if (r->status == 0 || r->status == 1) {
+    // not admitted: drop it from the queues now
+    for (auto* q : {&s->to_plan, &s->ready}) {
+      auto p = std::find(q->begin(), q->end(), r);
+      if (p != q->end()) q->erase(p);
+    }
+    r->status = VQC_ERR_CANCELED;
+    r->error = "request cancelled";
+    r->t_done = now_s();
+    s->cv_done.notify_all();
+  }
+  return 1;
 }
 
 int vqc_serve_stats(vqc_server s, long long* out) {

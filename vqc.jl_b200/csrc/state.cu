@@ -90,7 +90,7 @@ namespace {
 struct ProfRec {
   std::string cls;
   cudaEvent_t a, b;
-  double bytes;
+  double bytes, flops;
 };
 std::mutex g_prof_mu;
 bool g_prof_on = false;
@@ -98,15 +98,15 @@ std::vector<ProfRec> g_prof;
 struct ProfSum {
   std::string cls;
   long long launches = 0;
-  double ms = 0, bytes = 0;
+  double ms = 0, bytes = 0, flops = 0;
 };
 std::vector<ProfSum> g_prof_sum;
 }  // namespace
 
-ProfScope::ProfScope(cudaStream_t s, const char* cls, double bytes) : stream(s) {
+ProfScope::ProfScope(cudaStream_t s, const char* cls, double bytes, double flops) : stream(s) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   if (!g_prof_on) return;
-  ProfRec r{cls, nullptr, nullptr, bytes};
+  ProfRec r{cls, nullptr, nullptr, bytes, flops};
   if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) return;
   cudaEventRecord(r.a, s);
   token = (int)g_prof.size();
@@ -150,6 +150,7 @@ static void prof_collect() {
     t->launches += 1;
     t->ms += ms;
     t->bytes += r.bytes;
+    t->flops += r.flops;
   }
   g_prof.clear();
 }
@@ -472,6 +473,14 @@ int vqc_profile_get(int i, char* name, int name_len, long long* launches, double
   if (launches) *launches = t.launches;
   if (total_ms) *total_ms = t.ms;
   if (total_bytes) *total_bytes = t.bytes;
+  return VQC_OK;
+}
+
+int vqc_profile_flops(int i, double* total_flops) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  prof_collect();
+  if (i < 0 || i >= (int)g_prof_sum.size()) return fail(VQC_ERR_ARG, "profile index out of range");
+  if (total_flops) *total_flops = g_prof_sum[i].flops;
   return VQC_OK;
 }
 

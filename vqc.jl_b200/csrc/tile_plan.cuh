@@ -75,6 +75,7 @@ struct PassLoc {
   int nslots = 0;
   int row0 = 0;
   int64_t ntiles = 0;
+  double fma_ops = 0;  // FMA-pipe lane operations of the pass over the whole state
 };
 
 // A plan serialised for the device: one byte image holding every pass's

@@ -22,6 +22,13 @@ STATUS = {
 }
 
 
+class Cancelled(RuntimeError):
+    """VQC_ERR_CANCELED: the serving request was cancelled."""
+
+
+STATUS[-7] = Cancelled
+
+
 class VqcError(RuntimeError):
     pass
 
@@ -68,6 +75,8 @@ SIGNATURES = {
     "vqc_profile_enable": ([_I], _I),
     "vqc_profile_count": ([], _I),
     "vqc_profile_get": ([_I, ctypes.c_char_p, _I, ctypes.POINTER(ctypes.c_longlong), _D, _D], _I),
+    "vqc_profile_flops": ([_I, _D], _I),
+    "vqc_fma_peak": ([_I, _I, _D], _I),
     "vqc_apply_gate": ([_H, _I, _IP, _D], _I),
     "vqc_apply_circuit": ([_H, ctypes.POINTER(Gate_t), _I, _D, _I], _I),
     "vqc_expect_pauli": ([_H, ctypes.POINTER(Pauli_t), _I, _D], _I),
@@ -97,6 +106,7 @@ SIGNATURES = {
                           ctypes.POINTER(Pauli_t), _I, _I, _D, ctypes.POINTER(ctypes.c_int64)], _I),
     "vqc_serve_poll": ([_H, ctypes.c_int64, _D, _D], _I),
     "vqc_serve_wait": ([_H, ctypes.c_int64, _I, _D, _D], _I),
+    "vqc_serve_cancel": ([_H, ctypes.c_int64], _I),
     "vqc_serve_stats": ([_H, ctypes.POINTER(ctypes.c_longlong)], _I),
     "vqc_serve_timing": ([_H, _D], _I),
     "vqc_serve_loop_timing": ([_H, _D], _I),
@@ -132,8 +142,9 @@ def profile_enable(on):
     check(load().vqc_profile_enable(1 if on else 0))
 
 
-def profile_read():
-    """{kernel class: (launches, total_ms, total_algorithmic_bytes)}."""
+def profile_read(with_flops=False):
+    """{kernel class: (launches, total_ms, total_algorithmic_bytes)}, with a
+    fourth entry, the total FMA-pipe flops, when with_flops is set."""
     lib = load()
     out = {}
     for i in range(check(lib.vqc_profile_count())):
@@ -142,8 +153,20 @@ def profile_read():
         ms = ctypes.c_double()
         by = ctypes.c_double()
         check(lib.vqc_profile_get(i, name, 64, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by)))
-        out[name.value.decode()] = (n.value, ms.value, by.value)
+        rec = (n.value, ms.value, by.value)
+        if with_flops:
+            fl = ctypes.c_double()
+            check(lib.vqc_profile_flops(i, ctypes.byref(fl)))
+            rec = rec + (fl.value,)
+        out[name.value.decode()] = rec
     return out
+
+
+def fma_peak(device=0, kind=0):
+    """Measured FMA-pipe peak in TFLOP/s: kind 0 packed FP32, 1 scalar FP32, 2 FP64."""
+    out = ctypes.c_double()
+    check(load().vqc_fma_peak(device, kind, ctypes.byref(out)))
+    return out.value
 
 
 def exported_symbols():

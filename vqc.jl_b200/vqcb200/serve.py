@@ -86,6 +86,11 @@ class Server:
             return None
         return self._finish(t, e, lat)
 
+    def cancel(self, t):
+        """Cancel a request; True when it was cancelled, False when it had
+        already finished (its result can still be collected)."""
+        return _lib.check(self._lib.vqc_serve_cancel(self._h, t.id)) == 1
+
     def stats(self):
         out = (ctypes.c_longlong * 7)()
         _lib.check(self._lib.vqc_serve_stats(self._h, out))
