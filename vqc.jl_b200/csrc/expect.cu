@@ -253,6 +253,206 @@ __global__ void __launch_bounds__(kRedThreads)
   if (ACC) grid_reduce<2>(acc, s, res);
 }
 
+// Phase tables over 6-bit windows of the index.  The quad kernel above
+// evaluates every term of every group at every quad (a 64-bit mask, a
+// parity, a sign, two adds); here that work is done once, on the host.  A
+// group's phase at partner index j is
+//   f(j) = sum_w T_w[(j >> s_w) & 63] + sum_{t in no window} c_t (-1)^{|j & z_t|},
+//   T_w[u] = sum_{t in w} c_t (-1)^{|u & (z_t >> s_w)|},
+// where window w holds the terms whose whole z support lies in the bits
+// [s_w, s_w + 6) (the tables are summed in FP64 on the host and stored in the
+// state's precision; terms without Z have a constant phase, folded into a
+// table).  A window starting at bit 0 gives the four partners of a quad four
+// phases (entries u .. u+3, u a multiple of 4); a window starting at bit 2 or
+// above gives one phase for all four.  For the XXZ chain each flip-mask group
+// is one window, the diagonal group five.
+constexpr int kWinBits = 6, kWinSize = 1 << kWinBits;
+constexpr size_t kWinMaxTableBytes = 96 * 1024;
+struct DevGroupW {
+  uint64_t x;
+  int wbeg, wend;  // windows [wbeg, wend); window wbeg starts at bit 0 when low0
+  int tbeg, tend;  // terms in no window: signs evaluated per partner
+  int low0;
+  int pad;
+};
+
+template <class R, bool WRITE, bool ACC>
+__global__ void __launch_bounds__(kRedThreads)
+    k_pauli_win(const cplx<R>* __restrict__ bra, const cplx<R>* __restrict__ ket, cplx<R>* __restrict__ out,
+                int64_t N, const DevGroupW* __restrict__ groups, int ng, const int* __restrict__ shifts,
+                const cplx<R>* __restrict__ tables, int nw, const DevTerm* __restrict__ terms, int nt, double dfac,
+                Scratch s, double* res) {
+  using V = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  V* stab = reinterpret_cast<V*>(smem);
+  DevGroupW* sg = reinterpret_cast<DevGroupW*>(smem + sizeof(V) * (size_t)nw * kWinSize);
+  int* ssh = reinterpret_cast<int*>(sg + ng);
+  PTerm<R>* st = reinterpret_cast<PTerm<R>*>(ssh + ((nw + 3) & ~3));
+  for (int i = threadIdx.x; i < nw * kWinSize; i += blockDim.x) stab[i] = tables[i];
+  for (int i = threadIdx.x; i < ng; i += blockDim.x) sg[i] = groups[i];
+  for (int i = threadIdx.x; i < nw; i += blockDim.x) ssh[i] = shifts[i];
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+    const DevTerm t = terms[i];
+    st[i] = PTerm<R>{t.z, mkc<R>((R)t.c.x, (R)t.c.y), mkc<R>((R)t.c.x, (R)t.c.y)};
+  }
+  __syncthreads();
+  double acc[2] = {0, 0};
+  const V zero = mkc<R>(R(0), R(0));
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, nq4 = N >> 2;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nq4; k += stride) {
+    const int64_t i0 = k << 2;
+    V hv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) hv[a] = zero;
+    for (int gi = 0; gi < ng; ++gi) {
+      const DevGroupW& g = sg[gi];
+      const int64_t jb = i0 ^ (int64_t)(g.x & ~3ull);
+      V kv[4];
+      load4<R>(ket + jb, kv);
+      int w = g.wbeg;
+      V f = zero;
+      V W[4];
+      const bool four = g.low0 || g.tbeg < g.tend;
+      if (g.low0) {
+        const V* t = stab + (size_t)w * kWinSize + (jb & (kWinSize - 1));
+#pragma unroll
+        for (int b = 0; b < 4; ++b) W[b] = t[b];
+        ++w;
+      } else {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) W[b] = zero;
+      }
+      for (; w < g.wend; ++w) {
+        const V t = stab[(size_t)w * kWinSize + ((jb >> ssh[w]) & (kWinSize - 1))];
+        f.x += t.x;
+        f.y += t.y;
+      }
+      for (int q = g.tbeg; q < g.tend; ++q) {
+        const uint64_t m = (uint64_t)jb & st[q].z;
+        const int hb = (__popc((unsigned)m ^ (unsigned)(m >> 32)) & 1);
+        const V cc = st[q].c;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const bool odd = (hb ^ (__popc((unsigned)(b & st[q].z)) & 1)) != 0;
+          W[b].x += odd ? -cc.x : cc.x;
+          W[b].y += odd ? -cc.y : cc.y;
+        }
+      }
+      if (four) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) W[b].x += f.x, W[b].y += f.y;
+        switch ((int)(g.x & 3)) {  // (compile-time register indices)
+          case 0: pauli4_add<0>(hv, W, kv); break;
+          case 1: pauli4_add<1>(hv, W, kv); break;
+          case 2: pauli4_add<2>(hv, W, kv); break;
+          default: pauli4_add<3>(hv, W, kv); break;
+        }
+      } else {
+        switch ((int)(g.x & 3)) {
+          case 0: pauli4_add1<0>(hv, f, kv); break;
+          case 1: pauli4_add1<1>(hv, f, kv); break;
+          case 2: pauli4_add1<2>(hv, f, kv); break;
+          default: pauli4_add1<3>(hv, f, kv); break;
+        }
+      }
+    }
+    if (WRITE) {
+      const R df = (R)dfac;  // 1 or 2
+      if constexpr (sizeof(R) == 4) {
+        *reinterpret_cast<float4*>(out + i0) = make_float4(df * hv[0].x, df * hv[0].y, df * hv[1].x, df * hv[1].y);
+        *reinterpret_cast<float4*>(out + i0 + 2) = make_float4(df * hv[2].x, df * hv[2].y, df * hv[3].x, df * hv[3].y);
+      } else {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) out[i0 + a] = mkc<R>(df * hv[a].x, df * hv[a].y);
+      }
+    }
+    if (ACC) {
+      V b[4];
+      load4<R>(bra + i0, b);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const double2 bb = to_d2(b[a]), hh = to_d2(hv[a]);
+        acc[0] = fma(bb.x, hh.x, fma(bb.y, hh.y, acc[0]));
+        acc[1] = fma(bb.x, hh.y, fma(-bb.y, hh.x, acc[1]));
+      }
+    }
+  }
+  if (ACC) grid_reduce<2>(acc, s, res);
+}
+
+// Window tables of a prepared operator (terms grouped by flip mask; the
+// expectation's coefficients c).  Returns false when the tables would not fit
+// the kernel's shared memory (the quad kernel runs instead).
+struct PauliWin {
+  std::vector<DevGroupW> groups;
+  std::vector<int> shifts;
+  std::vector<cd> tables;  // nw * 64
+  std::vector<DevTerm> rest;
+};
+static bool build_windows(const std::vector<DevGroup>& groups, const std::vector<DevTerm>& terms, size_t amp_bytes,
+                          PauliWin& pw) {
+  for (const DevGroup& g : groups) {
+    std::vector<int> idx;
+    for (int t = g.start; t < g.start + g.count; ++t) idx.push_back(t);
+    auto lo_of = [&](int t) { return terms[t].z ? __builtin_ctzll(terms[t].z) : 0; };
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return lo_of(a) < lo_of(b); });
+    struct Win {
+      int s;
+      std::vector<cd> tab;
+    };
+    std::vector<Win> wins;
+    cd c0(0);
+    std::vector<DevTerm> rest;
+    for (int t : idx) {
+      const uint64_t z = terms[t].z;
+      const cd c(terms[t].c.x, terms[t].c.y);
+      if (!z) {
+        c0 += c;
+        continue;
+      }
+      const int lo = __builtin_ctzll(z), hi = 63 - __builtin_clzll(z);
+      Win* w = nullptr;
+      for (Win& x : wins)
+        if (x.s <= lo && hi < x.s + kWinBits) w = &x;
+      if (!w) {
+        int sh = -1;
+        if (hi < kWinBits)
+          sh = 0;
+        else if (lo >= 2 && hi - lo < kWinBits)
+          sh = lo;
+        if (sh < 0) {
+          rest.push_back(terms[t]);
+          continue;
+        }
+        wins.push_back(Win{sh, std::vector<cd>(kWinSize, cd(0))});
+        w = &wins.back();
+      }
+      const uint64_t zl = z >> w->s;
+      for (int u = 0; u < kWinSize; ++u) w->tab[u] += (__builtin_popcountll((uint64_t)u & zl) & 1) ? -c : c;
+    }
+    if (c0 != cd(0)) {
+      if (wins.empty()) wins.push_back(Win{2, std::vector<cd>(kWinSize, cd(0))});
+      for (cd& v : wins[0].tab) v += c0;
+    }
+    // the window at bit 0 (if any) first
+    std::stable_sort(wins.begin(), wins.end(), [](const Win& a, const Win& b) { return (a.s == 0) > (b.s == 0); });
+    DevGroupW d{};
+    d.x = g.x;
+    d.wbeg = (int)pw.shifts.size();
+    for (const Win& w : wins) {
+      pw.shifts.push_back(w.s);
+      pw.tables.insert(pw.tables.end(), w.tab.begin(), w.tab.end());
+    }
+    d.wend = (int)pw.shifts.size();
+    d.low0 = !wins.empty() && wins[0].s == 0;
+    d.tbeg = (int)pw.rest.size();
+    pw.rest.insert(pw.rest.end(), rest.begin(), rest.end());
+    d.tend = (int)pw.rest.size();
+    pw.groups.push_back(d);
+  }
+  return pw.tables.size() * amp_bytes <= kWinMaxTableBytes;
+}
+
 // tr(H rho) for a Pauli sum on a density matrix (expecs_dm.jl:19-30; the
 // reference sums tr(M_key rho_key) per position key, expec_dm_serial.jl).
 // With P|j> = c' (-1)^{|j & z|} |j ^ x> (the state-vector kernels' phase
@@ -323,11 +523,20 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
       if (write && first) VQC_CK(cudaMemsetAsync(out, 0, h->size() * h->amp_bytes(), h->stream));
       break;
     }
-    // quad kernel (n >= 2): terms of each group sorted by their low-bit class
+    // quad kernels (n >= 2): window tables when one coefficient set serves the
+    // expectation and the written operator and the tables fit; otherwise the
+    // terms of each group sorted by their low-bit class
     const bool quad = h->nq >= 2;
-    std::vector<DevGroup4> g4;
     bool sep = false;
-    if (quad) {
+    {
+      const double f = hermitian_part ? 2.0 : 1.0;
+      for (const DevTerm& t : p.terms)
+        if (t.d.x != f * t.c.x || t.d.y != f * t.c.y) sep = true;
+    }
+    PauliWin pw;
+    const bool win = quad && !sep && build_windows(p.groups, p.terms, h->amp_bytes(), pw);
+    std::vector<DevGroup4> g4;
+    if (quad && !win) {
       std::vector<DevTerm> sorted;
       for (const DevGroup& g : p.groups) {
         DevGroup4 q{};
@@ -341,21 +550,41 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
         g4.push_back(q);
       }
       p.terms.swap(sorted);
-      // one coefficient set unless the written operator is not a multiple of the expectation's
-      const double f = hermitian_part ? 2.0 : 1.0;
-      for (const DevTerm& t : p.terms)
-        if (t.d.x != f * t.c.x || t.d.y != f * t.c.y) sep = true;
     }
-    const size_t gb = quad ? sizeof(DevGroup4) * g4.size() : sizeof(DevGroup) * p.groups.size(),
-                 tb = sizeof(DevTerm) * p.terms.size();
-    std::vector<unsigned char> buf(gb + tb);
-    std::memcpy(buf.data(), quad ? (const void*)g4.data() : (const void*)p.groups.data(), gb);
-    std::memcpy(buf.data() + gb, p.terms.data(), tb);
+    // device image: [window tables][groups][shifts][terms in no window] for the
+    // window kernel, [groups][terms] otherwise
+    const size_t amp = h->amp_bytes();
+    const size_t wtb = win ? pw.tables.size() * amp : 0,
+                 gb = win ? sizeof(DevGroupW) * pw.groups.size()
+                          : (quad ? sizeof(DevGroup4) * g4.size() : sizeof(DevGroup) * p.groups.size()),
+                 shb = win ? sizeof(int) * ((pw.shifts.size() + 3) & ~size_t(3)) : 0,
+                 tb = sizeof(DevTerm) * (win ? pw.rest.size() : p.terms.size());
+    std::vector<unsigned char> buf(wtb + gb + shb + tb, 0);
+    if (win) {
+      for (size_t i = 0; i < pw.tables.size(); ++i) {
+        if (amp == 8) {
+          const float2 v = make_float2((float)pw.tables[i].real(), (float)pw.tables[i].imag());
+          std::memcpy(buf.data() + i * amp, &v, amp);
+        } else {
+          const double2 v = make_double2(pw.tables[i].real(), pw.tables[i].imag());
+          std::memcpy(buf.data() + i * amp, &v, amp);
+        }
+      }
+      std::memcpy(buf.data() + wtb, pw.groups.data(), gb);
+      if (!pw.shifts.empty()) std::memcpy(buf.data() + wtb + gb, pw.shifts.data(), sizeof(int) * pw.shifts.size());
+      if (tb) std::memcpy(buf.data() + wtb + gb + shb, pw.rest.data(), tb);
+    } else {
+      std::memcpy(buf.data(), quad ? (const void*)g4.data() : (const void*)p.groups.data(), gb);
+      std::memcpy(buf.data() + gb, p.terms.data(), tb);
+    }
     if ((rc = upload_ops(h, buf.data(), buf.size()))) return rc;
-    const DevGroup* dg = (const DevGroup*)h->opbuf;
-    const DevTerm* dt = (const DevTerm*)((unsigned char*)h->opbuf + gb);
-    const int ng = (int)p.groups.size(), nt = (int)p.terms.size();
-    const size_t smem = gb + tb;
+    const unsigned char* ob = (const unsigned char*)h->opbuf;
+    const DevGroup* dg = (const DevGroup*)(ob + wtb);
+    const DevTerm* dt = (const DevTerm*)(ob + wtb + gb + shb);
+    const int ng = (int)p.groups.size(), nt = (int)(win ? pw.rest.size() : p.terms.size());
+    const int nw = (int)pw.shifts.size();
+    const size_t smem = win ? wtb + gb + shb + pw.rest.size() * (amp == 8 ? sizeof(PTerm<float>) : sizeof(PTerm<double>))
+                            : gb + tb;
     const int grid = reduction_grid(h->device, h->size());
     // a later chunk accumulates onto `out`: run it into a workspace and add
     void* target = out;
@@ -368,7 +597,15 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
                    (double)h->size() * h->amp_bytes() * (1 + (write ? 1 : 0) + (acc && bra != ket ? 1 : 0)));
 #define VQC_PAULI_LAUNCH(R)                                                                                      \
   do {                                                                                                           \
-    if (quad) {                                                                                                  \
+    if (win) {                                                                                                   \
+      auto kfun = write ? (acc ? k_pauli_win<R, true, true> : k_pauli_win<R, true, false>)                       \
+                        : k_pauli_win<R, false, true>;                                                           \
+      if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+      kfun<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,   \
+                                                    h->size(), (const DevGroupW*)(ob + wtb), ng,                 \
+                                                    (const int*)(ob + wtb + gb), (const cplx<R>*)ob, nw, dt, nt, \
+                                                    hermitian_part ? 2.0 : 1.0, h->scr, h->scr.result);          \
+    } else if (quad) {                                                                                           \
       auto kfun = write ? (acc ? (sep ? k_pauli4<R, true, true, true> : k_pauli4<R, true, true, false>)          \
                                : (sep ? k_pauli4<R, true, false, true> : k_pauli4<R, true, false, false>))       \
                         : k_pauli4<R, false, true, false>;                                                       \
