@@ -129,6 +129,14 @@ int vqc_profile_get(int i, char* name, int name_len, long long* launches, double
  * (fused multiply-adds, multiplies, adds) the class's launches execute, for
  * the kernels bound by arithmetic (the tile passes); 0 for the others. */
 int vqc_profile_flops(int i, double* total_flops);
+/* Index checks of the debug build (libvqcb200_debug.so, compiled with
+ * VQC_DEBUG_CHECKS; no counterpart in the reference): the number of device
+ * accesses whose index fell outside its buffer since the last reset (each was
+ * skipped, not performed), and out[0..3] = (count, source line, index, limit)
+ * of the first.  reset != 0 clears the records.  Always 0 in the release
+ * build, which performs no checks; vqc_debug_build() tells which is loaded. */
+int vqc_debug_status(int reset, long long* out);
+int vqc_debug_build(void);
 /* Measured peak of the device's FMA pipe in TFLOP/s (2 flops per FMA lane):
  * a calibration kernel of independent FMA chains on every SM, timed with
  * CUDA events.  kind 0: packed two-lane FP32 (fma.rn.f32x2), 1: scalar

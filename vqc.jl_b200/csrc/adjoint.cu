@@ -45,6 +45,10 @@ __global__ void __launch_bounds__(kRedThreads)
 #pragma unroll
     for (int s = 0; s < MS; ++s)
       if (s < a.ns) {
+        if (!VQC_DCHECK(base + a.off[s], a.namp)) {
+          xl[s] = xp[s] = mkc<R>(R(0), R(0));
+          continue;
+        }
         xl[s] = lam[base + a.off[s]];
         xp[s] = psi[base + a.off[s]];
       }
@@ -60,6 +64,7 @@ __global__ void __launch_bounds__(kRedThreads)
           }
         yl[r] = al;
         yp[r] = ap;
+        if (!VQC_DCHECK(base + a.off[r], a.namp)) continue;
         lam[base + a.off[r]] = al;
         psi[base + a.off[r]] = ap;
       }

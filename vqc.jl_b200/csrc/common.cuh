@@ -16,6 +16,46 @@
 
 namespace vqc {
 
+// ----------------------------------------------------------------------------- debug checks
+// Built with -DVQC_DEBUG_CHECKS (vqcb200._build.build(debug=True), the
+// library libvqcb200_debug.so), every index wrapped in VQC_DCHECK(i, limit) is
+// tested on the device before its access: a violation increments this
+// translation unit's device record (keeping the first source line, index and
+// limit) and the access is skipped, so nothing traps and the context stays
+// usable.  vqc_debug_status() sums the records of every translation unit.
+// In the release build VQC_DCHECK is the constant true and compiles away.
+struct DebugRecord {
+  unsigned hits;
+  int line;
+  long long index, limit;
+};
+typedef int (*DebugReader)(DebugRecord* out, int reset);
+int register_debug_reader(DebugReader r);
+#ifdef VQC_DEBUG_CHECKS
+static __device__ DebugRecord g_vqc_dbg;
+__device__ __forceinline__ bool dcheck(long long i, long long lim, int line) {
+  if (i >= 0 && i < lim) return true;
+  if (atomicAdd(&g_vqc_dbg.hits, 1u) == 0u) {
+    g_vqc_dbg.line = line;
+    g_vqc_dbg.index = i;
+    g_vqc_dbg.limit = lim;
+  }
+  return false;
+}
+#define VQC_DCHECK(i, lim) (::vqc::dcheck((long long)(i), (long long)(lim), __LINE__))
+static int vqc_dbg_read(DebugRecord* out, int reset) {
+  if (cudaMemcpyFromSymbol(out, g_vqc_dbg, sizeof(DebugRecord)) != cudaSuccess) return -1;
+  if (reset) {
+    const DebugRecord z{};
+    if (cudaMemcpyToSymbol(g_vqc_dbg, &z, sizeof(z)) != cudaSuccess) return -1;
+  }
+  return 0;
+}
+[[maybe_unused]] static const int vqc_dbg_registered = register_debug_reader(&vqc_dbg_read);
+#else
+#define VQC_DCHECK(i, lim) true
+#endif
+
 // ----------------------------------------------------------------------------- complex
 template <class R>
 struct CT;

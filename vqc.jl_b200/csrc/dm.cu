@@ -91,6 +91,7 @@ __global__ void k_dm_ptrace(const cplx<R>* __restrict__ rho, int n, uint64_t kep
     double2 acc = make_double2(0, 0);
     for (int64_t c = 0; c < s2; ++c) {
       const int64_t t = deposit(c, traced);
+      if (!VQC_DCHECK((ra | t) + L * (cb | t), L * L)) continue;
       const double2 v = to_d2(rho[(ra | t) + L * (cb | t)]);
       acc.x += v.x;
       acc.y += v.y;
@@ -148,6 +149,10 @@ __global__ void __launch_bounds__(kRedThreads)
 #pragma unroll
     for (int t = 0; t < D; ++t) {
       const int64_t r = r0 + g.off[t];
+      if (!VQC_DCHECK(r + N * j, N * N) || !VQC_DCHECK(j + N * r, N * N)) {
+        bv[t] = make_double2(0, 0);
+        continue;
+      }
       bv[t] = dag_b ? to_d2(b[j + N * r]) : to_d2(b[r + N * j]);
       if (dag_b) bv[t].y = -bv[t].y;
     }

@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(kRedThreads)
     for (int gi = 0; gi < ng; ++gi) {
       const DevGroup g = sg[gi];
       const int64_t j = i ^ (int64_t)g.x;
+      if (!VQC_DCHECK(j, N)) continue;
       const double2 kv = to_d2(ket[j]);
       double2 f = make_double2(0, 0), fd = make_double2(0, 0);
       for (int q = g.start; q < g.start + g.count; ++q) {
@@ -181,6 +182,7 @@ __global__ void __launch_bounds__(kRedThreads)
     for (int gi = 0; gi < ng; ++gi) {
       const DevGroup4& g = sg[gi];
       const int64_t jb = i0 ^ (int64_t)(g.x & ~3ull);
+      if (!VQC_DCHECK(jb + 3, N)) continue;
       V kv[4];
       load4<R>(ket + jb, kv);
       if (g.cs[1] == g.cs[4]) {
@@ -307,6 +309,7 @@ __global__ void __launch_bounds__(kRedThreads)
     for (int gi = 0; gi < ng; ++gi) {
       const DevGroupW& g = sg[gi];
       const int64_t jb = i0 ^ (int64_t)(g.x & ~3ull);
+      if (!VQC_DCHECK(jb + 3, N)) continue;
       V kv[4];
       load4<R>(ket + jb, kv);
       int w = g.wbeg;

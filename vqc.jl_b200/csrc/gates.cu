@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(256) k_gate_sub(cplx<R>* __restrict__ v, const
     if (MODE == kDense) {
 #pragma unroll
       for (int s = 0; s < MS; ++s)
-        if (s < a.ns) x[s] = v[base + a.off[s]];
+        if (s < a.ns && VQC_DCHECK(base + a.off[s], a.namp)) x[s] = v[base + a.off[s]];
 #pragma unroll
       for (int r = 0; r < MS; ++r) {
         if (r < a.ns) {
@@ -105,20 +105,20 @@ __global__ void __launch_bounds__(256) k_gate_sub(cplx<R>* __restrict__ v, const
 #pragma unroll
           for (int c = 0; c < MS; ++c)
             if (c < a.ns) acc = cfma(a.U[r * MS + c], x[c], acc);
-          v[base + a.off[r]] = acc;
+          if (VQC_DCHECK(base + a.off[r], a.namp)) v[base + a.off[r]] = acc;
         }
       }
     } else if (MODE == kDiag) {
 #pragma unroll
       for (int s = 0; s < MS; ++s)
-        if (s < a.ns) v[base + a.off[s]] = cmul(a.U[s], v[base + a.off[s]]);
+        if (s < a.ns && VQC_DCHECK(base + a.off[s], a.namp)) v[base + a.off[s]] = cmul(a.U[s], v[base + a.off[s]]);
     } else {
 #pragma unroll
       for (int s = 0; s < MS; ++s)
-        if (s < a.ns) x[s] = v[base + a.src_off[s]];
+        if (s < a.ns && VQC_DCHECK(base + a.src_off[s], a.namp)) x[s] = v[base + a.src_off[s]];
 #pragma unroll
       for (int s = 0; s < MS; ++s)
-        if (s < a.ns) v[base + a.off[s]] = cmul(a.U[s], x[s]);
+        if (s < a.ns && VQC_DCHECK(base + a.off[s], a.namp)) v[base + a.off[s]] = cmul(a.U[s], x[s]);
     }
   }
 }

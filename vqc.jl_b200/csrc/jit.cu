@@ -173,7 +173,13 @@ int jit_mode() {
   return 1;
 }
 
+// The debug build (device-side index checks) runs every pass on the kernels
+// compiled into the library, whose checks it can read.
+#ifdef VQC_DEBUG_CHECKS
+bool jit_available() { return false; }
+#else
 bool jit_available() { return nvrtc().ok; }
+#endif
 
 // Resident CTAs per SM the compiled kernels' registers are budgeted for:
 // 1024 threads for forward passes (64 registers), 512 for the reverse sweep

@@ -133,6 +133,15 @@ void prof_note(const char* cls, long long count) {
   g_prof_sum.push_back(t);
 }
 
+std::vector<DebugReader>& debug_readers() {
+  static std::vector<DebugReader> r;
+  return r;
+}
+int register_debug_reader(DebugReader r) {
+  debug_readers().push_back(r);
+  return 0;
+}
+
 static void prof_collect() {
   for (auto& r : g_prof) {
     float ms = 0;
@@ -474,6 +483,32 @@ int vqc_profile_get(int i, char* name, int name_len, long long* launches, double
   if (total_ms) *total_ms = t.ms;
   if (total_bytes) *total_bytes = t.bytes;
   return VQC_OK;
+}
+
+int vqc_debug_status(int reset, long long* out) {
+  DebugRecord first{};
+  long long hits = 0;
+  for (DebugReader r : debug_readers()) {
+    DebugRecord d{};
+    if (r(&d, reset)) return fail(VQC_ERR_CUDA, "reading a debug record failed");
+    if (d.hits && !hits) first = d;
+    hits += d.hits;
+  }
+  if (out) {
+    out[0] = hits;
+    out[1] = first.line;
+    out[2] = first.index;
+    out[3] = first.limit;
+  }
+  return (int)std::min<long long>(hits, 1 << 30);
+}
+
+int vqc_debug_build(void) {
+#ifdef VQC_DEBUG_CHECKS
+  return 1;
+#else
+  return 0;
+#endif
 }
 
 int vqc_profile_flops(int i, double* total_flops) {

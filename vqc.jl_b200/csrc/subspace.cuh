@@ -9,6 +9,7 @@ namespace vqc {
 
 template <class R, int MS>
 struct SubArgs {
+  int64_t namp;  // amplitudes of the state (the debug build's index limit)
   int64_t ngroups;
   int64_t mask[6];
   int k;
@@ -30,6 +31,7 @@ __device__ __forceinline__ int64_t group_base(int64_t g, int k, const int64_t* m
 
 template <class R, int MS>
 void fill_sub_args(const GateSpec& g, int nq, SubArgs<R, MS>& a) {
+  a.namp = int64_t(1) << nq;
   a.ngroups = mask_of(g.k, g.sp, nq, a.mask);
   for (int j = g.k + 1; j < 6; ++j) a.mask[j] = 0;
   a.k = g.k;

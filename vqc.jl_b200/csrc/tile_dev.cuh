@@ -12,6 +12,12 @@ typedef int int32_t;
 #include <cstdint>
 #endif
 
+// Index checks of the debug build (common.cuh); the run-time compiled pass
+// kernels and the release build see the constant true.
+#ifndef VQC_DCHECK
+#define VQC_DCHECK(i, lim) true
+#endif
+
 namespace vqc {
 
 constexpr int kRegBits = 4;  // 16 amplitudes per thread

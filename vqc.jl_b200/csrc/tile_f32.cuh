@@ -749,6 +749,7 @@ __device__ __forceinline__ void stage_load(const TileCtx<M, ADJ>& x, const DevSt
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int64_t gi = g0 + S->gdep[m];
+      if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       const float4 t = *reinterpret_cast<const float4*>(x.psi + gi);
       v[m].r = mk(t.x, t.z);
       v[m].i = mk(t.y, t.w);
@@ -763,6 +764,7 @@ __device__ __forceinline__ void stage_load(const TileCtx<M, ADJ>& x, const DevSt
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint32_t a = sw ^ S->swm[m];
+      if (!VQC_DCHECK(a, (TileCtx<M, ADJ>::NPAIR))) continue;
       const ulonglong2 t = x.sp[a];
       v[m].r = t.x;
       v[m].i = t.y;
@@ -783,6 +785,7 @@ __device__ __forceinline__ void stage_store(const TileCtx<M, ADJ>& x, const DevS
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int64_t gi = g0 + S->gdep[m];
+      if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       *reinterpret_cast<float4*>(x.psi + gi) = make_float4(lo(v[m].r), lo(v[m].i), hi(v[m].r), hi(v[m].i));
       if (ADJ)
         *reinterpret_cast<float4*>(x.lam + gi) = make_float4(lo(w[m].r), lo(w[m].i), hi(w[m].r), hi(w[m].i));
@@ -792,6 +795,7 @@ __device__ __forceinline__ void stage_store(const TileCtx<M, ADJ>& x, const DevS
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint32_t a = sw ^ S->swm[m];
+      if (!VQC_DCHECK(a, (TileCtx<M, ADJ>::NPAIR))) continue;
       x.sp[a] = make_ulonglong2(v[m].r, v[m].i);
       if (ADJ) x.sl[a] = make_ulonglong2(w[m].r, w[m].i);
     }
@@ -808,6 +812,7 @@ __device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ>& x, const Dev
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int64_t gi = g0 + gdep[m];
+      if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       const float4 t = *reinterpret_cast<const float4*>(x.psi + gi);
       v[m].r = mk(t.x, t.z);
       v[m].i = mk(t.y, t.w);
@@ -822,6 +827,7 @@ __device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ>& x, const Dev
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint32_t a = sw ^ swm[m];
+      if (!VQC_DCHECK(a, (TileCtx<M, ADJ>::NPAIR))) continue;
       const ulonglong2 t = x.sp[a];
       v[m].r = t.x;
       v[m].i = t.y;
@@ -842,6 +848,7 @@ __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const De
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int64_t gi = g0 + gdep[m];
+      if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       *reinterpret_cast<float4*>(x.psi + gi) = make_float4(lo(v[m].r), lo(v[m].i), hi(v[m].r), hi(v[m].i));
       if (ADJ)
         *reinterpret_cast<float4*>(x.lam + gi) = make_float4(lo(w[m].r), lo(w[m].i), hi(w[m].r), hi(w[m].i));
@@ -851,6 +858,7 @@ __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const De
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint32_t a = sw ^ swm[m];
+      if (!VQC_DCHECK(a, (TileCtx<M, ADJ>::NPAIR))) continue;
       x.sp[a] = make_ulonglong2(v[m].r, v[m].i);
       if (ADJ) x.sl[a] = make_ulonglong2(w[m].r, w[m].i);
     }

@@ -304,6 +304,8 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
   }
   C v[16], w[16];
   const int s_first = P.stage_begin, s_last = P.stage_end - 1;
+  [[maybe_unused]] const int64_t namp = P.ntiles << M;  // the debug build's index limits
+  [[maybe_unused]] constexpr int64_t tsize = int64_t(1) << M;
   for (int64_t tile = blockIdx.x; tile < P.ntiles; tile += ncta) {
     const int64_t base = dep64(tile, P.nontile_mask);
     for (int s = s_first; s <= s_last; ++s) {
@@ -316,6 +318,7 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int64_t gi = g0 + (S->gdep[j]);
+          if (!VQC_DCHECK(gi, namp)) continue;
           v[j] = psi[gi];
           if (ADJ) w[j] = lam[gi];
         }
@@ -323,6 +326,7 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const uint32_t t = Swz<R>::f(tthr | dep[j]);
+          if (!VQC_DCHECK(t, tsize)) continue;
           v[j] = sp[t];
           if (ADJ) w[j] = sl[t];
         }
@@ -397,6 +401,7 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int64_t gi = g0 + (S->gdep[j]);
+          if (!VQC_DCHECK(gi, namp)) continue;
           psi[gi] = v[j];
           if (ADJ) lam[gi] = w[j];
         }
@@ -404,6 +409,7 @@ __device__ __forceinline__ void tile_body(cplx<R>* __restrict__ psi, cplx<R>* __
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const uint32_t t = Swz<R>::f(tthr | dep[j]);
+          if (!VQC_DCHECK(t, tsize)) continue;
           sp[t] = v[j];
           if (ADJ) sl[t] = w[j];
         }

@@ -7,7 +7,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libvqcb200.so")
+# VQC_DEBUG_LIB=1 loads the debug build (device-side index checks, see
+# vqc_debug_status in include/vqc_b200.h) instead of the release library
+LIB_PATH = os.path.join(HERE, "libvqcb200_debug.so" if os.environ.get("VQC_DEBUG_LIB") == "1" else "libvqcb200.so")
 
 VQC_C64 = 0
 VQC_C128 = 1
@@ -77,6 +79,8 @@ SIGNATURES = {
     "vqc_profile_get": ([_I, ctypes.c_char_p, _I, ctypes.POINTER(ctypes.c_longlong), _D, _D], _I),
     "vqc_profile_flops": ([_I, _D], _I),
     "vqc_fma_peak": ([_I, _I, _D], _I),
+    "vqc_debug_status": ([_I, ctypes.POINTER(ctypes.c_longlong)], _I),
+    "vqc_debug_build": ([], _I),
     "vqc_apply_gate": ([_H, _I, _IP, _D], _I),
     "vqc_apply_circuit": ([_H, ctypes.POINTER(Gate_t), _I, _D, _I], _I),
     "vqc_expect_pauli": ([_H, ctypes.POINTER(Pauli_t), _I, _D], _I),
@@ -160,6 +164,14 @@ def profile_read(with_flops=False):
             rec = rec + (fl.value,)
         out[name.value.decode()] = rec
     return out
+
+
+def debug_status(reset=False):
+    """(violations, first source line, first index, its limit) recorded by the
+    debug build's device-side index checks; (0, 0, 0, 0) in the release build."""
+    out = (ctypes.c_longlong * 4)()
+    check(load().vqc_debug_status(1 if reset else 0, out))
+    return tuple(out)
 
 
 def fma_peak(device=0, kind=0):
