@@ -69,3 +69,16 @@ def test_noalloc_rejects_too_many_terms():
     rc = lib.vqc_expect_pauli_noalloc(ctypes.c_void_p(buf.data_ptr()), 10, _lib.VQC_C128, arr, 1025, None, out)
     assert rc == -1
     assert b"1024" in lib.vqc_last_error()
+
+
+def test_noalloc_rejects_a_host_pointer():
+    """A host buffer is refused before any launch (a kernel given it would fault)."""
+    lib = V.load()
+    host = np.zeros(2 << 10, dtype=np.float64)
+    arr = (_lib.Pauli_t * 1)()
+    arr[0].zmask = 1
+    arr[0].coeff_re = 1.0
+    out = (ctypes.c_double * 2)()
+    rc = lib.vqc_expect_pauli_noalloc(ctypes.c_void_p(host.ctypes.data), 10, _lib.VQC_C128, arr, 1, None, out)
+    assert rc == -1
+    assert b"device" in lib.vqc_last_error()

@@ -1043,6 +1043,17 @@ extern "C" int vqc_expect_pauli_noalloc(const void* state, int nqubits, int dtyp
     return fail(VQC_ERR_ARG, "the allocation-free expectation takes at most 1024 Pauli terms per call");
   int device = 0;
   VQC_CK(cudaGetDevice(&device));
+  {
+    // the state must be device (or managed) memory of the current device: a
+    // host pointer or another GPU's buffer would fault the kernel
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, state) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(VQC_ERR_ARG, "state is not a CUDA device pointer");
+    }
+    if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != device)
+      return fail(VQC_ERR_ARG, "state must be device memory of the current device");
+  }
   unsigned char* base = noalloc_scratch_ptr(device);
   if (!base) return fail(VQC_ERR_CUDA, "cudaGetSymbolAddress of the static scratch array failed");
   cudaStream_t st = (cudaStream_t)stream;
@@ -1052,7 +1063,9 @@ extern "C" int vqc_expect_pauli_noalloc(const void* state, int nqubits, int dtyp
   }
   // group the terms by flip mask into a fixed-size table (no heap use)
   const uint64_t lim = nqubits >= 64 ? ~0ull : ((1ull << nqubits) - 1);
-  int order[kNoAllocMaxTerms];
+  // host tables in thread-local storage (not on the caller's stack, which
+  // may be small for the threads of such hosts)
+  static thread_local int order[kNoAllocMaxTerms];
   for (int i = 0; i < nterms; ++i) {
     if ((terms[i].xmask & ~lim) || (terms[i].zmask & ~lim)) return fail(VQC_ERR_ARG, "Pauli term acts outside the register");
     int j = i;
@@ -1061,7 +1074,7 @@ extern "C" int vqc_expect_pauli_noalloc(const void* state, int nqubits, int dtyp
   }
   // [groups][terms]: the terms are first written after room for nterms groups,
   // then moved down behind the ng groups actually used
-  alignas(16) unsigned char table[kNoAllocTableBytes];
+  alignas(16) static thread_local unsigned char table[kNoAllocTableBytes];
   DevGroup* groups = reinterpret_cast<DevGroup*>(table);
   DevTerm* dt = reinterpret_cast<DevTerm*>(table + sizeof(DevGroup) * nterms);
   int ng = 0;
