@@ -227,9 +227,13 @@ int vqc_dm_expect_pauli(vqc_state rho, const vqc_pauli* terms, int nterms, doubl
  * For callers that cannot allocate device memory (a fixed arena handed over
  * at start-up, no cudaMalloc/cudaFree afterwards): expectation(H, psi) of a
  * state in the caller's own device buffer `state` (2^nqubits amplitudes of
- * `dtype`, on the current device), on `stream` (a cudaStream_t, or NULL for
- * the default stream); out = (re, im) in FP64, the same quantity as
- * vqc_expect_pauli.  All scratch lives in one static device array of the
+ * `dtype`, device memory of the current device, else VQC_ERR_ARG), on
+ * `stream` (a cudaStream_t, or NULL for the default stream); out = (re, im)
+ * in FP64, the quantity vqc_expect_pauli computes, within rounding: this entry
+ * point runs the one-amplitude-per-thread Pauli kernel on a reduction grid of
+ * at most 296 blocks (its partial sums must fit the static array), so it is
+ * slower than vqc_expect_pauli on large states and sums in another order.
+ * Host tables live in thread-local storage, not on the caller's stack.  All scratch lives in one static device array of the
  * library (218,112 bytes per GPU that loads the library, held until exit);
  * at most 1024 Pauli terms per call (more: VQC_ERR_ARG).  The first call on a
  * device looks up the array's device address; make that first call before any

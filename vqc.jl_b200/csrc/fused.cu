@@ -852,7 +852,7 @@ static void note_plan(bool adj, const std::vector<PlanPass>& passes) {
 template <int M, bool ADJ>
 static int jit_grid(int device, const void* k, const PassShape& ps) {
   constexpr int NT = 1 << (M - kRegBits);
-  const size_t smem = pass_smem<float, M, ADJ>(ps);
+  const size_t smem = pass_smem<float, M, ADJ>(ps) + jit_extra_smem(ADJ, M);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem) != cudaSuccess || per_sm < 1) {
@@ -867,7 +867,7 @@ static int launch_tile_jit(vqc_state h, const void* k, void* psi, void* lam, con
                            const DevOp* dops, const void* pool, double* partials, int grid, const PassShape& ps,
                            const void* host_pool, double flops) {
   constexpr int NT = 1 << (M - kRegBits);
-  const size_t smem = pass_smem<float, M, ADJ>(ps);
+  const size_t smem = pass_smem<float, M, ADJ>(ps) + jit_extra_smem(ADJ, M);
   VQC_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
   ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward", (double)(ADJ ? 4 : 2) * h->size() * sizeof(float2),
                  flops);

@@ -181,6 +181,14 @@ bool jit_available() { return false; }
 bool jit_available() { return nvrtc().ok; }
 #endif
 
+// Forward passes with the asynchronous tile copy (VQC_JIT_ASYNC, default on):
+// a second tile buffer in shared memory receives the next tile by cp.async
+// while the current tile is computed.
+bool jit_async_fwd() { return env_int("VQC_JIT_ASYNC", 1) != 0; }
+size_t jit_extra_smem(bool adj, int M) {
+  return (!adj && jit_async_fwd() && env_int("VQC_JIT_BAKE", 1)) ? (size_t(1) << (M - 1)) * 16 : 0;
+}
+
 // Resident CTAs per SM the compiled kernels' registers are budgeted for:
 // 1024 threads for forward passes (64 registers), 512 for the reverse sweep
 // (128 registers).
@@ -193,6 +201,8 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
   if (npool > kJitMaxCoef) return std::string();  // beyond the kernel-parameter space: interpreter
   std::ostringstream os;
   const int NT = 1 << (M - kRegBits);
+  const bool bake = env_int("VQC_JIT_BAKE", 1) != 0;
+  const bool async = jit_extra_smem(adj, M) > 0;
   // the pass's matrix pool travels as a kernel parameter (constant bank,
   // read uniformly by the whole grid) instead of through shared memory
   os << "#include \"tile_f32.cuh\"\n"
@@ -205,13 +215,33 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
      << "  constexpr int NW = TileCtx<M, ADJ>::NW;\n"
      << "  __shared__ DevPass P;\n  __shared__ uint64_t s_inc, s_base0;\n"
      << "  TileCtx<M, ADJ> x;\n"
-     << "  tile_setup<M, ADJ>(x, psi, lam, pass, stages, ops, pool, gridDim.x, P, s_inc, s_base0, false);\n"
-     << "  Pk v[8], w[8];\n"
-     << "  for (int it = 0; it < x.ntiles_here; ++it) {\n";
-  const bool bake = env_int("VQC_JIT_BAKE", 1) != 0;
+     << "  tile_setup<M, ADJ" << (async ? ", 2" : "")
+     << ">(x, psi, lam, pass, stages, ops, pool, gridDim.x, P, s_inc, s_base0, false);\n"
+     << "  Pk v[8], w[8];\n";
+  if (async) {
+    // the first stage's pair offsets, for the copies of the next tile
+    os << "  constexpr uint32_t swm0[8] = {";
+    for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[0].swm[m] << "u";
+    os << "};\n  constexpr int64_t gdep0[8] = {";
+    for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[0].gdep[m] << "ll";
+    os << "};\n  ulonglong2* tbuf[2] = {x.sp, x.spb};\n"
+       << "  if (x.ntiles_here > 0) tile_copy_async<M>(x, x.stages, x.base, tbuf[0], swm0, gdep0);\n";
+  }
+  os << "  for (int it = 0; it < x.ntiles_here; ++it) {\n";
+  if (async)
+    os << "    if (it + 1 < x.ntiles_here) {\n"
+       << "      tile_copy_async<M>(x, x.stages, tile_base_after(x, s_inc), tbuf[(it + 1) & 1], swm0, gdep0);\n"
+       << "      cp_async_wait<1>();\n    } else {\n      cp_async_wait<0>();\n    }\n"
+       << "    __syncthreads();\n    x.sp = tbuf[it & 1];\n";
   for (int s = 0; s < nst; ++s) {
     os << "  {\n    const DevStageF* S = x.stages + " << s << ";\n";
-    if (bake) {
+    if (async && s == 0) {
+      os << "    constexpr uint32_t swm[8] = {";
+      for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[s].swm[m] << "u";
+      os << "};\n    constexpr int64_t gdep[8] = {";
+      for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[s].gdep[m] << "ll";
+      os << "};\n    stage_load_raw<M>(x, S, x.sp, v, swm);\n";
+    } else if (bake) {
       // the stage's pair offsets as constants (they depend on the pass's qubits)
       os << "    constexpr uint32_t swm[8] = {";
       for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[s].swm[m] << "u";
@@ -221,10 +251,13 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
     } else {
       os << "    stage_load<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w);\n";
     }
-    if (s == 0 && bake && env_int("VQC_JIT_L2PF", 1))
+    if (s == 0 && bake && !async && env_int("VQC_JIT_L2PF", 1))
       os << "    if (it + 1 < x.ntiles_here) prefetch_next_l2<M, ADJ>(x, S, s_inc, gdep);\n";
     os << "    const uint32_t tthr = S->thr[0][x.tlo] | S->thr[1][x.thi];\n    (void)tthr;\n";
     for (int o = st[s].op_begin; o < st[s].op_end; ++o) emit_op(os, ops[o], o);
+    // the first stage of an asynchronous pass read its input from the buffer it
+    // now writes (in the next stage's layout): every read must be done first
+    if (async && s == 0 && nst > 1) os << "    __syncthreads();\n";
     if (bake)
       os << "    stage_store_k<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w, swm, gdep);\n  }\n";
     else
@@ -329,7 +362,8 @@ std::map<std::pair<uint64_t, uint64_t>, const void*>& hcache() {
 int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out) {
   out.assign(refs.size(), nullptr);
   if (!jit_available()) return VQC_OK;
-  const int flags[4] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M), M};
+  const int flags[5] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M), M,
+                        (int)jit_extra_smem(adj, M)};
   std::vector<std::pair<uint64_t, uint64_t>> keys(refs.size());
   std::vector<size_t> miss;
   {

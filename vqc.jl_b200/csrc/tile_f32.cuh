@@ -671,6 +671,7 @@ struct TileCtx {
   float2* lam;
   ulonglong2* sp;
   ulonglong2* sl;
+  ulonglong2* spb;  // the second tile buffer of the asynchronous forward passes (NBUF = 2)
   double* sacc;
   const DevStageF* stages;
   const DevOp* ops;
@@ -681,16 +682,20 @@ struct TileCtx {
 };
 
 // Stages the pass's descriptors, zeroes the accumulation slots and sets up
-// the tile counter.  Every thread of the CTA calls it.
-template <int M, bool ADJ>
+// the tile counter.  Every thread of the CTA calls it.  NBUF = 2 puts a
+// second tile buffer in front of the usual layout (the asynchronous forward
+// passes copy the next tile into it while the current one is computed).
+template <int M, bool ADJ, int NBUF = 1>
 __device__ __forceinline__ void tile_setup(TileCtx<M, ADJ>& x, float2* psi, float2* lam, const DevPass* pass,
                                            const DevStageF* stages, const DevOp* ops, const float2* pool, int ncta,
                                            DevPass& P, uint64_t& s_inc, uint64_t& s_base0, bool stage_pool = true) {
   constexpr int NT = TileCtx<M, ADJ>::NT, NW = TileCtx<M, ADJ>::NW, NPAIR = TileCtx<M, ADJ>::NPAIR;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem_all[];
+  unsigned char* smem = smem_all + (NBUF - 1) * (unsigned long long)NPAIR * 16;
   if (threadIdx.x == 0) P = *pass;
   __syncthreads();
   const int nslots = ADJ ? P.nslots : 0;
+  x.spb = reinterpret_cast<ulonglong2*>(smem_all);
   x.sp = reinterpret_cast<ulonglong2*>(smem);
   x.sl = x.sp + (ADJ ? NPAIR : 0);
   x.sacc = reinterpret_cast<double*>(smem + tile_bytes_f32<M, ADJ>());
@@ -864,6 +869,55 @@ __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const De
     }
   }
   __syncthreads();
+}
+
+// ----------------------------------------------------------------------------- asynchronous tile copies
+// Forward passes: the next tile's first-stage pairs are copied into a second
+// shared buffer with cp.async (16 bytes per pair, as stored in HBM: two
+// interleaved complex amplitudes) while the current tile is computed, so the
+// HBM transfer overlaps the arithmetic instead of following it.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+template <int M, bool ADJ>
+__device__ __forceinline__ uint64_t tile_base_after(const TileCtx<M, ADJ>& x, uint64_t s_inc) {
+  return ((x.base | ~x.P->nontile_mask) + s_inc) & x.P->nontile_mask;
+}
+// The first stage's pairs of the tile at `base` into `buf`, at the stage's
+// swizzled pair indices; one commit group per tile.
+template <int M>
+__device__ __forceinline__ void tile_copy_async(const TileCtx<M, false>& x, const DevStageF* S, uint64_t base,
+                                                ulonglong2* buf, const uint32_t (&swm)[8], const int64_t (&gdep)[8]) {
+  const int64_t g0 = (int64_t)base + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
+  const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int64_t gi = g0 + gdep[m];
+    const uint32_t a = sw ^ swm[m];
+    if (!VQC_DCHECK(gi + 1, x.P->ntiles << M) || !VQC_DCHECK(a, (TileCtx<M, false>::NPAIR))) continue;
+    cp_async16(buf + a, x.psi + gi);
+  }
+  cp_async_commit();
+}
+// The first stage's registers from that copy (interleaved -> packed pairs).
+template <int M>
+__device__ __forceinline__ void stage_load_raw(const TileCtx<M, false>& x, const DevStageF* S, const ulonglong2* buf,
+                                               Pk (&v)[8], const uint32_t (&swm)[8]) {
+  const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const uint32_t a = sw ^ swm[m];
+    if (!VQC_DCHECK(a, (TileCtx<M, false>::NPAIR))) continue;
+    const float4 t = reinterpret_cast<const float4*>(buf)[a];
+    v[m].r = mk(t.x, t.z);
+    v[m].i = mk(t.y, t.w);
+  }
 }
 
 // L2 prefetch of the next tile's first-stage pairs (no shared memory, no

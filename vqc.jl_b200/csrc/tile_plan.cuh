@@ -143,6 +143,9 @@ struct ReqPlan {
 int jit_mode();        // 0 off, 1 on, 2 auto, 3 packed interpreter (VQC_JIT)
 bool jit_available();  // NVRTC could be loaded
 int jit_min_blocks(bool adj, int M);
+// Shared-memory bytes a compiled pass needs beyond pass_smem (the second tile
+// buffer of the asynchronous forward passes).
+size_t jit_extra_smem(bool adj, int M);
 // Source of a pass's kernel ("" when the pass is not compiled: its matrix
 // pool, passed as a kernel parameter, would exceed kJitMaxCoef entries).
 constexpr int kJitMaxCoef = 3800;
