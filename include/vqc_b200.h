@@ -251,8 +251,9 @@ int vqc_expect_pauli_noalloc(const void* state, int nqubits, int dtype, const vq
  * same quantities as vqc_adjoint_grad).  Admission is by device memory: a
  * request is admitted when its states, descriptors and scratch fit
  * `memory_bytes` and fewer than `max_active` requests run.  Every loop
- * iteration advances every admitted request by one step, all steps of a kind
- * in one launch; requests arriving meanwhile join at the next iteration.  A
+ * iteration advances every admitted request by one step, the steps of a kind
+ * in few launches (FP32 passes on run-time compiled kernels, one launch per
+ * pass structure); requests arriving meanwhile join at the next iteration.  A
  * request's result does not depend on the requests it is batched with. */
 typedef struct vqc_server_s* vqc_server;
 int vqc_serve_open(int device, int dtype, size_t memory_bytes, int max_active, int planner_threads,

@@ -53,20 +53,55 @@ def test_serve_matches_single_path_and_oracle():
 
 
 def test_same_result_alone_and_in_the_mix():
+    """A request's result does not depend on what it is batched with: within
+    the FP32 bound (1e-5) on an FP32 server (a request of 2^18+ amplitudes may
+    run on the generic or on a compiled kernel, depending on whether its pass
+    structure was compiled when it was planned), and bit for bit on an FP64
+    server (one kernel for every request)."""
     rng = np.random.default_rng(51)
     mix = []
     for i in range(16):
         n = int(rng.integers(9, 19))
         spec, hspec = make_request(rng, n, int(rng.integers(2, 7)))
         mix.append((n, spec, hspec))
-    probe = mix[5]
-    with Server(dtype=np.complex64, memory_bytes=2 << 30, max_active=64) as srv:
-        t = srv.submit(probe[0], W.to_circuit(probe[1]), W.to_operator(probe[2]), want_grad=True)
-        alone = srv.wait(t)
-        ts = [srv.submit(n, W.to_circuit(s), W.to_operator(h), want_grad=True) for n, s, h in mix]
-        in_mix = [srv.wait(x) for x in ts][5]
-    assert alone[0] == in_mix[0]
-    assert np.array_equal(alone[1], in_mix[1])
+    for dtype in (np.complex64, np.complex128):
+        for probe_i in (5, max(range(16), key=lambda i: mix[i][0])):
+            probe = mix[probe_i]
+            with Server(dtype=dtype, memory_bytes=2 << 30, max_active=64) as srv:
+                t = srv.submit(probe[0], W.to_circuit(probe[1]), W.to_operator(probe[2]), want_grad=True)
+                alone = srv.wait(t)
+                ts = [srv.submit(n, W.to_circuit(s), W.to_operator(h), want_grad=True) for n, s, h in mix]
+                in_mix = [srv.wait(x) for x in ts][probe_i]
+            if dtype == np.complex128:
+                assert alone[0] == in_mix[0]
+                assert np.array_equal(alone[1], in_mix[1])
+            else:
+                assert abs(alone[0] - in_mix[0]) <= 1e-5 * abs(in_mix[0])
+                assert rel(alone[1], in_mix[1]) < 1e-5
+
+
+def test_compiled_batch_kernels_match_oracle():
+    """Requests of 2^18 or more amplitudes run on batch kernels compiled for
+    their pass structure once it has been compiled (by a planner thread, after
+    the first request of that structure was handed on to run on the generic
+    kernel).  A cold and a warm round of one structure both match the oracle."""
+    rng = np.random.default_rng(59)
+    n = 18
+    reqs = [make_request(rng, n, 3) for _ in range(4)]
+    with Server(dtype=np.complex64, memory_bytes=1 << 30, max_active=8) as srv:
+        cold = srv.wait(srv.submit(n, W.to_circuit(reqs[0][0]), W.to_operator(reqs[0][1])))
+        time.sleep(10)  # the structure's kernels compile meanwhile
+        ts = [srv.submit(n, W.to_circuit(sp), W.to_operator(h), want_grad=bool(i % 2 == 0)) for i, (sp, h) in
+              enumerate(reqs)]
+        warm = [srv.wait(t) for t in ts]
+    for (sp, h), (e, g, _), want in [(reqs[0], cold, True)] + [(r, o, i % 2 == 0) for i, (r, o) in
+                                                              enumerate(zip(reqs, warm))]:
+        e_ref, g_ref = O.energy_and_gradient(O.from_spec(sp), O.terms_from_spec(h), O.zero_state(n), nthreads=8)
+        assert abs(e - e_ref) / max(abs(e_ref), 1.0) < 1e-5
+        if want:
+            assert rel(g, g_ref) < 1e-5
+        else:
+            assert g is None
 
 
 def test_requests_arriving_while_others_run():

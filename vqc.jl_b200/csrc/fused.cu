@@ -1177,10 +1177,12 @@ __global__ void __launch_bounds__(256) k_reduce_slots_batch(const RedItem* __res
 
 template <class R, int M>
 static int build_plan_tm(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
-                         const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp) {
+                         const std::vector<std::vector<ParamInfo>>& params, bool want_grad, bool packed,
+                         ReqPlan& rp) {
   const TileConfig tc = tile_config(dtype, n);
-  auto shape_max = [](const SerialPlan& sp) {
+  auto shape_max = [packed](const SerialPlan& sp) {
     PassShape m;
+    m.packed = packed;
     for (const PassLoc& l : sp.locs) {
       m.nslots = std::max(m.nslots, l.shape.nslots);
       m.nstages = std::max(m.nstages, l.shape.nstages);
@@ -1198,7 +1200,7 @@ static int build_plan_tm(int n, int dtype, const std::vector<GateSpec>& fspecs, 
   plan_passes(n, tc, false, items, passes);
   for (const PlanPass& p : passes)
     if (p.standalone) return fail(VQC_ERR_UNSUPPORTED, "serving takes gates with at most two target qubits");
-  serialize_plan<R, M, false>(n, dtype, passes, rp.fwd, nullptr);
+  serialize_plan<R, M, false>(n, dtype, passes, rp.fwd, nullptr, packed);
   rp.fwd_max = shape_max(rp.fwd);
   if (want_grad) {
     std::vector<PItem> ritems = reverse_items(rspecs, params);
@@ -1207,7 +1209,7 @@ static int build_plan_tm(int n, int dtype, const std::vector<GateSpec>& fspecs, 
     for (const PlanPass& p : rpasses)
       if (p.standalone)
         return fail(VQC_ERR_UNSUPPORTED, "serving takes parameterised gates with one target qubit (or diagonal)");
-    serialize_plan<R, M, true>(n, dtype, rpasses, rp.adj, &rp.accs);
+    serialize_plan<R, M, true>(n, dtype, rpasses, rp.adj, &rp.accs, packed);
     rp.adj_max = shape_max(rp.adj);
   }
   rp.M = M;
@@ -1215,18 +1217,95 @@ static int build_plan_tm(int n, int dtype, const std::vector<GateSpec>& fspecs, 
   return VQC_OK;
 }
 
-int serve_build_plan(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
-                     const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp) {
-  if (n < kMinTileBits || n > 40) return fail(VQC_ERR_UNSUPPORTED, "serving takes 9 to 40 qubits");
+static int build_plan_any(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
+                          const std::vector<std::vector<ParamInfo>>& params, bool want_grad, bool packed,
+                          ReqPlan& rp) {
   switch (tile_config(dtype, n).M + (dtype == VQC_C64 ? 0 : 100)) {
-    case 12: return build_plan_tm<float, 12>(n, dtype, fspecs, rspecs, params, want_grad, rp);
-    case 11: return build_plan_tm<float, 11>(n, dtype, fspecs, rspecs, params, want_grad, rp);
-    case 10: return build_plan_tm<float, 10>(n, dtype, fspecs, rspecs, params, want_grad, rp);
-    case 9: return build_plan_tm<float, 9>(n, dtype, fspecs, rspecs, params, want_grad, rp);
-    case 111: return build_plan_tm<double, 11>(n, dtype, fspecs, rspecs, params, want_grad, rp);
-    case 110: return build_plan_tm<double, 10>(n, dtype, fspecs, rspecs, params, want_grad, rp);
-    default: return build_plan_tm<double, 9>(n, dtype, fspecs, rspecs, params, want_grad, rp);
+    case 12: return build_plan_tm<float, 12>(n, dtype, fspecs, rspecs, params, want_grad, packed, rp);
+    case 11: return build_plan_tm<float, 11>(n, dtype, fspecs, rspecs, params, want_grad, packed, rp);
+    case 10: return build_plan_tm<float, 10>(n, dtype, fspecs, rspecs, params, want_grad, packed, rp);
+    case 9: return build_plan_tm<float, 9>(n, dtype, fspecs, rspecs, params, want_grad, packed, rp);
+    case 111: return build_plan_tm<double, 11>(n, dtype, fspecs, rspecs, params, want_grad, false, rp);
+    case 110: return build_plan_tm<double, 10>(n, dtype, fspecs, rspecs, params, want_grad, false, rp);
+    default: return build_plan_tm<double, 9>(n, dtype, fspecs, rspecs, params, want_grad, false, rp);
   }
+}
+
+// The compiled batch kernels of a packed plan's passes (false when one has
+// none); compile = false only looks them up.
+static bool plan_kernels(int M, bool adj, const SerialPlan& sp, std::vector<const void*>& ks, bool compile) {
+  std::vector<JitPassRef> refs(sp.locs.size());
+  for (size_t i = 0; i < sp.locs.size(); ++i)
+    refs[i] = JitPassRef{(const DevStageF*)(sp.buf.data() + sp.locs[i].stages), sp.locs[i].shape.nstages,
+                         (const DevOp*)(sp.buf.data() + sp.locs[i].ops), sp.locs[i].shape.npool};
+  if (jit_pass_kernels(M, adj, refs, ks, true, compile)) return false;
+  for (const void* k : ks)
+    if (!k) return false;
+  return true;
+}
+
+// Serving compiles the passes of requests of at least 2^18 amplitudes (where
+// the device time of a mix concentrates); smaller requests share the generic
+// kernel's single launch per step kind.
+constexpr int kServeJitMinQubits = 18;
+
+int serve_build_plan(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
+                     const std::vector<std::vector<ParamInfo>>& params, bool want_grad, bool compiled, ReqPlan& rp,
+                     ReqPlan* to_compile) {
+  if (n < kMinTileBits || n > 40) return fail(VQC_ERR_UNSUPPORTED, "serving takes 9 to 40 qubits");
+  if (compiled && dtype == VQC_C64 && n >= kServeJitMinQubits && jit_available()) {
+    int rc = build_plan_any(n, dtype, fspecs, rspecs, params, want_grad, true, rp);
+    if (rc) return rc;
+    if (plan_kernels(rp.M, false, rp.fwd, rp.fwd_k, false) &&
+        (!want_grad || plan_kernels(rp.M, true, rp.adj, rp.adj_k, false)))
+      return VQC_OK;
+    // not compiled yet: this request runs the classic plan on the generic kernel
+    if (to_compile) *to_compile = std::move(rp);
+    rp = ReqPlan();
+  }
+  return build_plan_any(n, dtype, fspecs, rspecs, params, want_grad, false, rp);
+}
+
+void serve_compile_plan(const ReqPlan& packed, bool want_grad) {
+  std::vector<const void*> ks;
+  plan_kernels(packed.M, false, packed.fwd, ks, true);
+  if (want_grad) plan_kernels(packed.M, true, packed.adj, ks, true);
+}
+
+// Shared memory of a compiled FP32 pass of shape ps (the formula of pass_smem).
+static size_t jit_pass_smem(int M, bool adj, const PassShape& ps) {
+  const size_t nt = size_t(1) << (M - kRegBits);
+  const size_t npool = (size_t)ps.npool * sizeof(float2);
+  return (adj ? 2 : 1) * (size_t(1) << M) * sizeof(float2) + (adj ? (size_t)ps.nslots * (nt / 32) * 8 * sizeof(double) : 0) +
+         sizeof(DevStageF) * ps.nstages + sizeof(DevOp) * ps.nops + ((npool + 15) & ~size_t(15));
+}
+
+int serve_jit_gridx(int M, bool adj, const std::vector<const void*>& ks, const SerialPlan& sp, int64_t ntiles,
+                    int device) {
+  int per_sm = 1 << 20;
+  for (size_t i = 0; i < ks.size(); ++i) {
+    const size_t smem = jit_pass_smem(M, adj, sp.locs[i].shape);
+    cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, ks[i], 1 << (M - kRegBits), smem) != cudaSuccess || b < 1) {
+      cudaGetLastError();
+      b = 1;
+    }
+    per_sm = std::min(per_sm, b);
+  }
+  if (ks.empty()) per_sm = 1;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)device_info(device).sms * per_sm));
+}
+
+int serve_launch_jit(int M, bool adj, const void* kernel, const TileItem* d_items, int nitems, int gridx,
+                     const PassShape& maxs, cudaStream_t stream) {
+  const size_t smem = jit_pass_smem(M, adj, maxs);
+  VQC_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)std::max<size_t>(smem, 48 * 1024)));
+  ProfScope prof(stream, adj ? "serve_tile_adjoint" : "serve_tile_forward", 0);
+  void* args[] = {(void*)&d_items};
+  VQC_CK(cudaLaunchKernel(kernel, dim3(gridx, nitems), dim3(1 << (M - kRegBits)), args, smem, stream));
+  return VQC_OK;
 }
 
 template <class R, int M, bool ADJ>

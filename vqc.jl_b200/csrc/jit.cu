@@ -27,6 +27,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <sstream>
 #include <thread>
 
@@ -121,8 +122,9 @@ bool compile_one(const std::string& src, std::vector<char>& cubin, std::string& 
   return ok;
 }
 
-// The code of one op of a stage (o = its index in the pass's op array).
-void emit_op(std::ostringstream& os, const DevOp& op, int o) {
+// The code of one op of a stage (o = its index in the pass's op array; cx =
+// the expression of the pass's coefficient array).
+void emit_op(std::ostringstream& os, const DevOp& op, int o, const char* cx) {
   const int code = op.code, type = code & 15;
   const bool ctl = code & kCodeCtl, gctl = code & kCodeGCtl, acc = code & kCodeAcc;
   os << "    { const DevOp* op = x.ops + " << o << ";\n";
@@ -130,7 +132,7 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o) {
   if (type == kOpU1) {
     const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = acc_kind_of(code);
     const int cb = rctl == 0 ? -1 : rctl - 1;
-    os << "      const u64* c = coef.c + " << op.mat << ";\n";
+    os << "      const u64* c = " << cx << " + " << op.mat << ";\n";
     if (ctl) os << "      const bool run = (tthr & op->cmask) == op->cval;\n";
     if (acc) os << "      float s8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};\n";
     os << "      " << (ctl ? "if (run) " : "") << "{\n";
@@ -149,10 +151,10 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o) {
   } else if (type == kOpU2) {
     const int ja = (code >> 4) & 3, jb = (code >> 6) & 3;
     if (ctl) os << "      if ((tthr & op->cmask) == op->cval)\n";
-    os << "      u2_op<" << ja << ", " << jb << ", ADJ>(v, w, reinterpret_cast<const float2*>(coef.c + " << op.mat
+    os << "      u2_op<" << ja << ", " << jb << ", ADJ>(v, w, reinterpret_cast<const float2*>(" << cx << " + " << op.mat
        << "), (uint32_t)op->rmask);\n";
   } else if (type == kOpDiag) {
-    os << "      diag_op<ADJ>(v, w, op, reinterpret_cast<const float2*>(coef.c + " << op.mat
+    os << "      diag_op<ADJ>(v, w, op, reinterpret_cast<const float2*>(" << cx << " + " << op.mat
        << "), tthr, S->dep, x.base);\n";
   } else {
     os << "      float s8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};\n"
@@ -181,43 +183,65 @@ bool jit_available() { return false; }
 bool jit_available() { return nvrtc().ok; }
 #endif
 
-// Forward passes with the asynchronous tile copy (VQC_JIT_ASYNC, default on):
-// a second tile buffer in shared memory receives the next tile by cp.async
-// while the current tile is computed.
-bool jit_async_fwd() { return env_int("VQC_JIT_ASYNC", 1) != 0; }
+// Forward passes with the asynchronous tile copy (VQC_JIT_ASYNC=1; off by
+// default): a second tile buffer in shared memory receives the next tile by
+// cp.async while the current tile is computed.  Measured at n = 26: 0.43 ms
+// per forward pass against 0.355 ms for the default (three resident CTAs
+// instead of four, and one more barrier per tile, cost more than the copy
+// saves; the default already prefetches the next tile into L2).
+bool jit_async_fwd() { return env_int("VQC_JIT_ASYNC", 0) != 0; }
 size_t jit_extra_smem(bool adj, int M) {
   return (!adj && jit_async_fwd() && env_int("VQC_JIT_BAKE", 1)) ? (size_t(1) << (M - 1)) * 16 : 0;
 }
 
 // Resident CTAs per SM the compiled kernels' registers are budgeted for:
-// 1024 threads for forward passes (64 registers), 512 for the reverse sweep
-// (128 registers).
+// 1024 threads for forward passes (64 registers), 768 when they hold a second
+// tile buffer (85 registers: their shared memory admits three 256-thread CTAs
+// anyway), 512 for the reverse sweep (128 registers).
 int jit_min_blocks(bool adj, int M) {
   const int nt = 1 << (M - kRegBits);
-  return adj ? env_int("VQC_JIT_MINB_ADJ", 512 / nt) : env_int("VQC_JIT_MINB_FWD", 1024 / nt);
+  if (adj) return env_int("VQC_JIT_MINB_ADJ", 512 / nt);
+  return env_int("VQC_JIT_MINB_FWD", (jit_async_fwd() && env_int("VQC_JIT_BAKE", 1) ? 768 : 1024) / nt);
 }
 
-std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool) {
-  if (npool > kJitMaxCoef) return std::string();  // beyond the kernel-parameter space: interpreter
+std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool, bool batch) {
+  if (!batch && npool > kJitMaxCoef) return std::string();  // beyond the kernel-parameter space: interpreter
   std::ostringstream os;
   const int NT = 1 << (M - kRegBits);
   const bool bake = env_int("VQC_JIT_BAKE", 1) != 0;
-  const bool async = jit_extra_smem(adj, M) > 0;
-  // the pass's matrix pool travels as a kernel parameter (constant bank,
-  // read uniformly by the whole grid) instead of through shared memory
+  const bool async = !batch && jit_extra_smem(adj, M) > 0;
   os << "#include \"tile_f32.cuh\"\n"
-     << "using namespace vqc;\nusing namespace vqc::f32t;\n"
-     << "struct Coef { unsigned long long c[" << std::max(npool, 2) << "]; };\n"
-     << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M) << ")\n"
-     << "vqc_pass(float2* psi, float2* lam, const DevPass* pass, const DevStageF* stages, const DevOp* ops,\n"
-     << "         const float2* pool, double* partials, const __grid_constant__ Coef coef) {\n"
-     << "  constexpr int M = " << M << ";\n  constexpr bool ADJ = " << (adj ? "true" : "false") << ";\n"
+     << "using namespace vqc;\nusing namespace vqc::f32t;\n";
+  if (!batch) {
+    // the pass's matrix pool travels as a kernel parameter (constant bank,
+    // read uniformly by the whole grid) instead of through shared memory
+    os << "struct Coef { unsigned long long c[" << std::max(npool, 2) << "]; };\n"
+       << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M) << ")\n"
+       << "vqc_pass(float2* psi, float2* lam, const DevPass* pass, const DevStageF* stages, const DevOp* ops,\n"
+       << "         const float2* pool, double* partials, const __grid_constant__ Coef coef) {\n"
+       << "  const int ncta = gridDim.x;\n";
+  } else {
+    // the serving loop: one request per blockIdx.y, each with its own state,
+    // descriptors and coefficient pool (staged in shared memory)
+    os << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M) << ")\n"
+       << "vqc_pass_batch(const TileItem* __restrict__ items) {\n"
+       << "  const TileItem item = items[blockIdx.y];\n"
+       << "  if ((int)blockIdx.x >= item.ncta) return;\n"
+       << "  const int ncta = item.ncta;\n"
+       << "  float2* psi = (float2*)item.psi;\n  float2* lam = (float2*)item.lam;\n"
+       << "  const DevPass* pass = item.pass;\n  const DevStageF* stages = (const DevStageF*)item.stages;\n"
+       << "  const DevOp* ops = item.ops;\n  const float2* pool = (const float2*)item.pool;\n"
+       << "  double* partials = item.partials;\n";
+  }
+  os << "  constexpr int M = " << M << ";\n  constexpr bool ADJ = " << (adj ? "true" : "false") << ";\n"
      << "  constexpr int NW = TileCtx<M, ADJ>::NW;\n"
      << "  __shared__ DevPass P;\n  __shared__ uint64_t s_inc, s_base0;\n"
      << "  TileCtx<M, ADJ> x;\n"
      << "  tile_setup<M, ADJ" << (async ? ", 2" : "")
-     << ">(x, psi, lam, pass, stages, ops, pool, gridDim.x, P, s_inc, s_base0, false);\n"
+     << ">(x, psi, lam, pass, stages, ops, pool, ncta, P, s_inc, s_base0, " << (batch ? "true" : "false") << ");\n"
      << "  Pk v[8], w[8];\n";
+  if (batch) os << "  const u64* C = reinterpret_cast<const u64*>(x.pool);\n";
+  const char* cx = batch ? "C" : "coef.c";
   if (async) {
     // the first stage's pair offsets, for the copies of the next tile
     os << "  constexpr uint32_t swm0[8] = {";
@@ -254,7 +278,7 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
     if (s == 0 && bake && !async && env_int("VQC_JIT_L2PF", 1))
       os << "    if (it + 1 < x.ntiles_here) prefetch_next_l2<M, ADJ>(x, S, s_inc, gdep);\n";
     os << "    const uint32_t tthr = S->thr[0][x.tlo] | S->thr[1][x.thi];\n    (void)tthr;\n";
-    for (int o = st[s].op_begin; o < st[s].op_end; ++o) emit_op(os, ops[o], o);
+    for (int o = st[s].op_begin; o < st[s].op_end; ++o) emit_op(os, ops[o], o, cx);
     // the first stage of an asynchronous pass read its input from the buffer it
     // now writes (in the next stage's layout): every read must be done first
     if (async && s == 0 && nst > 1) os << "    __syncthreads();\n";
@@ -269,7 +293,7 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
 
 // Kernels for `srcs` (nullptr where unavailable): cached ones at once, the
 // rest compiled in parallel, then loaded.
-int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out) {
+int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out, const char* name) {
   out.assign(srcs.size(), nullptr);
   if (!jit_available()) return VQC_OK;
   std::vector<size_t> todo;
@@ -314,7 +338,7 @@ int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& 
       e.log = logs[k];
       if (ok[k] && cudaLibraryLoadData(&e.lib, bins[k].data(), nullptr, nullptr, 0, nullptr, nullptr, 0) ==
                        cudaSuccess &&
-          cudaLibraryGetKernel(&e.kernel, e.lib, "vqc_pass") == cudaSuccess) {
+          cudaLibraryGetKernel(&e.kernel, e.lib, name) == cudaSuccess) {
         e.failed = false;
       } else {
         e.failed = true;
@@ -359,18 +383,26 @@ std::map<std::pair<uint64_t, uint64_t>, const void*>& hcache() {
 }
 }  // namespace
 
-int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out) {
+// Structures some thread is compiling now: another thread that misses them
+// does not compile them again (it gets nullptr, the interpreter's case).
+std::set<std::pair<uint64_t, uint64_t>>& inflight() {
+  static std::set<std::pair<uint64_t, uint64_t>> s;
+  return s;
+}
+
+int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out, bool batch,
+                     bool compile) {
   out.assign(refs.size(), nullptr);
   if (!jit_available()) return VQC_OK;
-  const int flags[5] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M), M,
-                        (int)jit_extra_smem(adj, M)};
+  const int flags[6] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M), M,
+                        batch ? 0 : (int)jit_extra_smem(adj, M), batch ? 1 : 0};
   std::vector<std::pair<uint64_t, uint64_t>> keys(refs.size());
   std::vector<size_t> miss;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     for (size_t i = 0; i < refs.size(); ++i) {
       const JitPassRef& r = refs[i];
-      if (!r.stages || r.npool > kJitMaxCoef) continue;
+      if (!r.stages || (!batch && r.npool > kJitMaxCoef)) continue;
       Hash128 h;
       h.add(flags, sizeof(flags));
       h.val(adj);
@@ -391,23 +423,27 @@ int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::
       auto it = hcache().find(keys[i]);
       if (it != hcache().end())
         out[i] = it->second;
-      else
+      else if (compile && !inflight().count(keys[i]) &&
+               std::find_if(miss.begin(), miss.end(), [&](size_t m) { return keys[m] == keys[i]; }) == miss.end())
         miss.push_back(i);
     }
+    for (size_t m : miss) inflight().insert(keys[m]);
   }
   if (miss.empty()) return VQC_OK;
   std::vector<std::string> srcs(miss.size());
   for (size_t k = 0; k < miss.size(); ++k) {
     const JitPassRef& r = refs[miss[k]];
-    srcs[k] = jit_pass_source(M, adj, r.stages, r.nstages, r.ops, r.npool);
+    srcs[k] = jit_pass_source(M, adj, r.stages, r.nstages, r.ops, r.npool, batch);
   }
   std::vector<const void*> ks;
-  int rc = jit_kernels(srcs, ks);
-  if (rc) return rc;
+  int rc = jit_kernels(srcs, ks, batch ? "vqc_pass_batch" : "vqc_pass");
   std::lock_guard<std::mutex> lk(g_mu);
-  for (size_t k = 0; k < miss.size(); ++k) {
-    out[miss[k]] = ks[k];
-    hcache()[keys[miss[k]]] = ks[k];  // (nullptr: compiled and failed; the interpreter runs it)
+  for (size_t m : miss) inflight().erase(keys[m]);
+  if (rc) return rc;
+  for (size_t k = 0; k < miss.size(); ++k) hcache()[keys[miss[k]]] = ks[k];  // (nullptr: failed; the interpreter runs it)
+  for (size_t i = 0; i < refs.size(); ++i) {  // every pass of a structure compiled here (duplicates too)
+    auto it = hcache().find(keys[i]);
+    if (!out[i] && it != hcache().end()) out[i] = it->second;
   }
   return VQC_OK;
 }

@@ -9,8 +9,11 @@
 //      count allows; a request that never fits is rejected;
 //   2. take the next step of EVERY admitted request -- a forward pass, the
 //      Pauli pass (energy, and the cotangent (H + H^dagger) psi), a reverse
-//      pass -- and run all steps of one kind as ONE launch (a 2-D grid:
-//      request x tiles), whatever the requests' qubit counts;
+//      pass -- and launch the steps of a kind together (a 2-D grid: request x
+//      tiles): FP32 tile passes grouped by pass structure, one launch of that
+//      structure's compiled kernel per group (the planner threads compile each
+//      structure once; requests of one qubit count share most structures),
+//      the others on the generic tile kernel in one launch per tile size;
 //   3. wait for the launches, retire finished requests (results to the host,
 //      memory back to the budget) and loop.
 // Requests that arrive while others run are admitted at the next iteration,
@@ -28,6 +31,7 @@
 #include <map>
 #include <memory>
 #include <thread>
+#include <tuple>
 
 #include "engine.h"
 #include "tile_plan.cuh"
@@ -57,6 +61,7 @@ struct Request {
   double* grads_out = nullptr;
   // plan
   ReqPlan plan;
+  ReqPlan to_compile;  // a packed plan whose kernels the planner compiles after handing the request on
   std::vector<unsigned char> image;  // fwd plan | adj plan | pauli tables
   size_t off_adj = 0, off_pauli = 0;
   int ng = 0, nt = 0;
@@ -136,7 +141,10 @@ static int plan_request(vqc_server_s* s, Request& r) {
                              (int)r.params.size(), rspecs, per_gate);
     if (rc) return rc;
   }
-  int rc = serve_build_plan(r.n, s->dtype, fspecs, rspecs, per_gate, r.grad, r.plan);
+  // FP32 requests run on compiled batch kernels (one per pass structure,
+  // compiled here in the planner thread the first time a structure is seen)
+  // unless run-time compilation is off (VQC_JIT=off) or fails
+  int rc = serve_build_plan(r.n, s->dtype, fspecs, rspecs, per_gate, r.grad, jit_mode() != 0, r.plan, &r.to_compile);
   if (rc) return rc;
   std::vector<unsigned char> pimg;
   if ((rc = serve_pauli_image(r.n, r.terms.data(), (int)r.terms.size(), true, pimg, r.ng, r.nt))) return rc;
@@ -150,8 +158,13 @@ static int plan_request(vqc_server_s* s, Request& r) {
   r.pauli_smem = pimg.size();
   const int64_t N = int64_t(1) << r.n;
   r.pauli_cap = (int)std::min<int64_t>((N + kRedThreads - 1) / kRedThreads, device_info(s->device).sms * 2);
-  r.fwd_cap = serve_tile_gridx(s->dtype, r.plan.M, false, r.plan.fwd_max, r.plan.ntiles, s->device);
-  r.adj_cap = r.grad ? serve_tile_gridx(s->dtype, r.plan.M, true, r.plan.adj_max, r.plan.ntiles, s->device) : 0;
+  r.fwd_cap = r.plan.fwd_k.empty()
+                  ? serve_tile_gridx(s->dtype, r.plan.M, false, r.plan.fwd_max, r.plan.ntiles, s->device)
+                  : serve_jit_gridx(r.plan.M, false, r.plan.fwd_k, r.plan.fwd, r.plan.ntiles, s->device);
+  r.adj_cap = !r.grad ? 0
+              : r.plan.adj_k.empty()
+                  ? serve_tile_gridx(s->dtype, r.plan.M, true, r.plan.adj_max, r.plan.ntiles, s->device)
+                  : serve_jit_gridx(r.plan.M, true, r.plan.adj_k, r.plan.adj, r.plan.ntiles, s->device);
   const size_t amp = s->dtype == VQC_C64 ? 8 : 16;
   size_t off = 0;
   auto take = [&](size_t b) {
@@ -190,25 +203,32 @@ static void planner_main(vqc_server_s* s) {
       s->to_plan.pop_front();
     }
     const int rc = plan_request(s, *r);
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (r->status < 0) {
-      // cancelled while it was being planned
-    } else if (rc) {
-      r->status = rc;
-      r->error = vqc_last_error();
-      r->t_done = now_s();
-      s->cv_done.notify_all();
-    } else if (r->dbytes > s->budget) {
-      r->status = VQC_ERR_BUSY;
-      r->error = "request needs more device memory than the serving budget";
-      r->t_done = now_s();
-      s->cv_done.notify_all();
-    } else {
-      r->status = 1;
-      r->t_planned = now_s();
-      s->ready.push_back(r);
-      s->cv_ready.notify_all();
+    ReqPlan compile_later;
+    std::swap(compile_later, r->to_compile);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (r->status < 0) {
+        // cancelled while it was being planned
+      } else if (rc) {
+        r->status = rc;
+        r->error = vqc_last_error();
+        r->t_done = now_s();
+        s->cv_done.notify_all();
+      } else if (r->dbytes > s->budget) {
+        r->status = VQC_ERR_BUSY;
+        r->error = "request needs more device memory than the serving budget";
+        r->t_done = now_s();
+        s->cv_done.notify_all();
+      } else {
+        r->status = 1;
+        r->t_planned = now_s();
+        s->ready.push_back(r);
+        s->cv_ready.notify_all();
+      }
     }
+    // the request is on its way; compile its structure for the next ones
+    // (other planner threads meanwhile plan other requests)
+    if (!compile_later.fwd.locs.empty()) serve_compile_plan(compile_later, !compile_later.adj.locs.empty());
   }
 }
 
@@ -318,86 +338,57 @@ static void worker_main(vqc_server_s* s) {
     if (s->active.empty()) continue;
     // 2. one launch per step kind (and tile size) over every active request
     const double t_build = now_s();
-    std::vector<TileItem> fwd_items[13], adj_items[13];
+    // tile items grouped by (tile size, direction, compiled kernel or the generic one)
+    struct Group {
+      std::vector<TileItem> items;
+      std::vector<std::shared_ptr<Request>> reqs;
+      std::vector<const PassLoc*> locs;
+      unsigned char* d = nullptr;
+    };
+    std::map<std::tuple<int, int, const void*>, Group> groups;
     std::vector<RedItem> red_items;
     std::vector<PauliItem> p_items[2];  // [0] energy only, [1] energy + cotangent
     std::vector<PauliRed> p_red[2];
-    std::vector<std::shared_ptr<Request>> fwd_req[13], adj_req[13];
     for (auto& r : s->active) {
       const int F = r->nfwd();
       const unsigned char* img = r->dimg;
       if (r->step < F) {
         const PassLoc& l = r->plan.fwd.locs[r->step];
-        fwd_items[r->plan.M].push_back(TileItem{r->psi, nullptr, (const DevPass*)(img + l.pass),
-                                                (const void*)(img + l.stages), (const DevOp*)(img + l.ops),
-                                                img + r->plan.fwd.pool_off + l.pool_begin * amp, nullptr, l.ntiles,
-                                                r->fwd_cap, 0});
-        fwd_req[r->plan.M].push_back(r);
+        const void* k = r->plan.fwd_k.empty() ? nullptr : r->plan.fwd_k[r->step];
+        Group& g = groups[std::make_tuple(r->plan.M, 0, k)];
+        g.items.push_back(TileItem{r->psi, nullptr, (const DevPass*)(img + l.pass), (const void*)(img + l.stages),
+                                   (const DevOp*)(img + l.ops), img + r->plan.fwd.pool_off + l.pool_begin * amp,
+                                   nullptr, l.ntiles, r->fwd_cap, 0});
+        g.reqs.push_back(r);
+        g.locs.push_back(&l);
       } else if (r->step == F) {
         const unsigned char* pt = img + r->off_pauli;
         p_items[r->grad].push_back(PauliItem{r->psi, r->lam, int64_t(1) << r->n, (const DevGroup*)pt, r->ng,
                                              (const DevTerm*)(pt + sizeof(DevGroup) * r->ng), r->nt, r->partials});
         p_red[r->grad].push_back(PauliRed{r->partials, 0, r->energy_dev});
       } else {
-        const PassLoc& l = r->plan.adj.locs[r->step - F - 1];
+        const int st = r->step - F - 1;
+        const PassLoc& l = r->plan.adj.locs[st];
         const unsigned char* ai = img + r->off_adj;
-        adj_items[r->plan.M].push_back(TileItem{r->psi, r->lam, (const DevPass*)(ai + l.pass),
-                                                (const void*)(ai + l.stages), (const DevOp*)(ai + l.ops),
-                                                ai + r->plan.adj.pool_off + l.pool_begin * amp, r->partials,
-                                                l.ntiles, r->adj_cap, 0});
-        adj_req[r->plan.M].push_back(r);
+        const void* k = r->plan.adj_k.empty() ? nullptr : r->plan.adj_k[st];
+        Group& g = groups[std::make_tuple(r->plan.M, 1, k)];
+        g.items.push_back(TileItem{r->psi, r->lam, (const DevPass*)(ai + l.pass), (const void*)(ai + l.stages),
+                                   (const DevOp*)(ai + l.ops), ai + r->plan.adj.pool_off + l.pool_begin * amp,
+                                   r->partials, l.ntiles, r->adj_cap, 0});
+        g.reqs.push_back(r);
+        g.locs.push_back(&l);
+        if (l.nslots > 0)
+          red_items.push_back(RedItem{r->partials, r->adj_cap, l.nslots, r->rows + (size_t)l.row0 * 8});
       }
     }
     // stage every item array in one pinned buffer, one copy
     size_t need = 0;
     auto add = [&](size_t b) { need = ((need + 15) & ~size_t(15)) + b; };
-    for (int M = 0; M < 13; ++M) {
-      add(sizeof(TileItem) * fwd_items[M].size());
-      add(sizeof(TileItem) * adj_items[M].size());
-    }
+    for (auto& kv : groups) add(sizeof(TileItem) * kv.second.items.size());
     add(sizeof(PauliItem) * p_items[0].size());
     add(sizeof(PauliItem) * p_items[1].size());
-    // reduce items depend on the launch grid: build them after the grids are known
-    std::vector<int> adj_gridx(13, 0), fwd_gridx(13, 0);
     int p_gridx = 0;
     size_t p_smem = 0;
-    for (int M = 0; M < 13; ++M) {
-      if (!fwd_items[M].empty()) {
-        PassShape mx;
-        int64_t mt = 0;
-        for (size_t i = 0; i < fwd_items[M].size(); ++i) {
-          const auto& r = fwd_req[M][i];
-          const PassShape& sh = r->plan.fwd.locs[r->step].shape;
-          mx.nstages = std::max(mx.nstages, sh.nstages);
-          mx.nops = std::max(mx.nops, sh.nops);
-          mx.npool = std::max(mx.npool, sh.npool);
-          mt = std::max(mt, fwd_items[M][i].ntiles);
-        }
-        (void)mt;
-        for (const TileItem& it : fwd_items[M]) fwd_gridx[M] = std::max(fwd_gridx[M], it.ncta);
-      }
-      if (!adj_items[M].empty()) {
-        int64_t mt = 0;
-        PassShape mx;
-        for (size_t i = 0; i < adj_items[M].size(); ++i) {
-          const auto& r = adj_req[M][i];
-          const PassShape& sh = r->plan.adj.locs[r->step - r->nfwd() - 1].shape;
-          mx.nslots = std::max(mx.nslots, sh.nslots);
-          mx.nstages = std::max(mx.nstages, sh.nstages);
-          mx.nops = std::max(mx.nops, sh.nops);
-          mx.npool = std::max(mx.npool, sh.npool);
-          mt = std::max(mt, adj_items[M][i].ntiles);
-        }
-        (void)mt;
-        for (const TileItem& it : adj_items[M]) adj_gridx[M] = std::max(adj_gridx[M], it.ncta);
-        for (size_t i = 0; i < adj_items[M].size(); ++i) {
-          const auto& r = adj_req[M][i];
-          const PassLoc& l = r->plan.adj.locs[r->step - r->nfwd() - 1];
-          if (l.nslots > 0)
-            red_items.push_back(RedItem{r->partials, r->adj_cap, l.nslots, r->rows + (size_t)l.row0 * 8});
-        }
-      }
-    }
     for (int v = 0; v < 2; ++v)
       for (size_t i = 0; i < p_items[v].size(); ++i) {
         const int64_t N = p_items[v][i].N;
@@ -429,12 +420,7 @@ static void worker_main(vqc_server_s* s) {
       pos += b;
       return s->d_items + o;
     };
-    unsigned char* d_fwd[13];
-    unsigned char* d_adj[13];
-    for (int M = 0; M < 13; ++M) {
-      d_fwd[M] = put(fwd_items[M].data(), sizeof(TileItem) * fwd_items[M].size());
-      d_adj[M] = put(adj_items[M].data(), sizeof(TileItem) * adj_items[M].size());
-    }
+    for (auto& kv : groups) kv.second.d = put(kv.second.items.data(), sizeof(TileItem) * kv.second.items.size());
     unsigned char* d_p[2];
     unsigned char* d_pred[2];
     for (int v = 0; v < 2; ++v) {
@@ -444,25 +430,38 @@ static void worker_main(vqc_server_s* s) {
     unsigned char* d_red = put(red_items.data(), sizeof(RedItem) * red_items.size());
     SRV_CK(cudaMemcpyAsync(s->d_items, s->h_items, pos, cudaMemcpyHostToDevice, s->stream));
     long long nl = 0, ni = 0;
-    for (int M = 0; M < 13; ++M) {
-      if (!fwd_items[M].empty()) {
+    // forward groups, the Pauli passes, then the reverse groups (a request takes one step per iteration)
+    auto launch_groups = [&](int adj) -> bool {
+      for (auto& kv : groups) {
+        if (std::get<1>(kv.first) != adj) continue;
+        const int M = std::get<0>(kv.first);
+        const void* k = std::get<2>(kv.first);
+        Group& g = kv.second;
         PassShape mx;
-        for (size_t i = 0; i < fwd_items[M].size(); ++i) {
-          const auto& r = fwd_req[M][i];
-          const PassShape& sh = r->plan.fwd.locs[r->step].shape;
+        mx.packed = k != nullptr;
+        int gridx = 0;
+        for (size_t i = 0; i < g.items.size(); ++i) {
+          const PassShape& sh = g.locs[i]->shape;
+          mx.nslots = std::max(mx.nslots, sh.nslots);
           mx.nstages = std::max(mx.nstages, sh.nstages);
           mx.nops = std::max(mx.nops, sh.nops);
           mx.npool = std::max(mx.npool, sh.npool);
+          gridx = std::max(gridx, g.items[i].ncta);
         }
-        if (serve_launch_tiles(s->dtype, M, false, (const TileItem*)d_fwd[M], (int)fwd_items[M].size(), fwd_gridx[M],
-                               mx, s->stream)) {
+        const int rc = k ? serve_launch_jit(M, adj != 0, k, (const TileItem*)g.d, (int)g.items.size(), gridx, mx,
+                                            s->stream)
+                         : serve_launch_tiles(s->dtype, M, adj != 0, (const TileItem*)g.d, (int)g.items.size(),
+                                              gridx, mx, s->stream);
+        if (rc) {
           fail_all(s, vqc_last_error());
-          return;
+          return false;
         }
         ++nl;
-        ni += (long long)fwd_items[M].size();
+        ni += (long long)g.items.size();
       }
-    }
+      return true;
+    };
+    if (!launch_groups(0)) return;
     for (int v = 0; v < 2; ++v) {
       if (p_items[v].empty()) continue;
       if (serve_launch_pauli(s->dtype, v == 1, (const PauliItem*)d_p[v], (int)p_items[v].size(), p_gridx, p_smem,
@@ -474,26 +473,7 @@ static void worker_main(vqc_server_s* s) {
       ++nl;
       ni += (long long)p_items[v].size();
     }
-    for (int M = 0; M < 13; ++M) {
-      if (!adj_items[M].empty()) {
-        PassShape mx;
-        for (size_t i = 0; i < adj_items[M].size(); ++i) {
-          const auto& r = adj_req[M][i];
-          const PassShape& sh = r->plan.adj.locs[r->step - r->nfwd() - 1].shape;
-          mx.nslots = std::max(mx.nslots, sh.nslots);
-          mx.nstages = std::max(mx.nstages, sh.nstages);
-          mx.nops = std::max(mx.nops, sh.nops);
-          mx.npool = std::max(mx.npool, sh.npool);
-        }
-        if (serve_launch_tiles(s->dtype, M, true, (const TileItem*)d_adj[M], (int)adj_items[M].size(), adj_gridx[M],
-                               mx, s->stream)) {
-          fail_all(s, vqc_last_error());
-          return;
-        }
-        ++nl;
-        ni += (long long)adj_items[M].size();
-      }
-    }
+    if (!launch_groups(1)) return;
     if (!red_items.empty()) {
       int ms = 0;
       for (auto& it : red_items) ms = std::max(ms, it.nslots);

@@ -90,6 +90,23 @@ __host__ __device__ constexpr int acc_kind_of(int code) {
   return ((code >> 14) & 3) | ((code & kCodeAH) ? kAccAH : 0);
 }
 
+// One pass each of many states in one launch (the serving path): request
+// blockIdx.y, its tiles strided over its own `ncta` CTAs (fixed per request,
+// so its sums are grouped the same way whatever it is batched with); CTAs
+// beyond ncta leave at once.
+struct TileItem {
+  void* psi;
+  void* lam;
+  const DevPass* pass;
+  const void* stages;  // DevStage (FP64) or DevStageF (FP32)
+  const DevOp* ops;
+  const void* pool;
+  double* partials;  // [ncta][nslots][8]
+  int64_t ntiles;
+  int ncta;
+  int pad;
+};
+
 // Shared-memory bytes of the FP32 tile(s) of one pass.
 template <int M, bool ADJ>
 __host__ __device__ constexpr unsigned long long tile_bytes_f32() {

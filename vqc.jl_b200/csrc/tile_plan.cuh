@@ -18,22 +18,6 @@ __host__ __device__ constexpr size_t tile_bytes() {
   return (size_t)(ADJ ? 2 : 1) * (size_t(1) << M) * sizeof(cplx<R>);
 }
 
-// One pass each of many states in one launch (the serving path): request
-// blockIdx.y, its tiles strided over its own `ncta` CTAs (fixed per request,
-// so its sums are grouped the same way whatever it is batched with); CTAs
-// beyond ncta leave at once.
-struct TileItem {
-  void* psi;
-  void* lam;
-  const DevPass* pass;
-  const void* stages;  // DevStage (FP64) or DevStageF (FP32)
-  const DevOp* ops;
-  const void* pool;
-  double* partials;  // [ncta][nslots][8]
-  int64_t ntiles;
-  int ncta;
-  int pad;
-};
 
 struct PGrad {
   int param;             // caller's parameter index
@@ -137,6 +121,8 @@ struct ReqPlan {
   std::vector<AccRef> accs;
   PassShape fwd_max, adj_max;
   int64_t ntiles = 0;
+  // compiled batch kernels per pass (FP32 packed plans), empty for the generic kernel
+  std::vector<const void*> fwd_k, adj_k;
 };
 
 // Run-time specialised FP32 tile kernels (jit.cu).
@@ -149,9 +135,10 @@ size_t jit_extra_smem(bool adj, int M);
 // Source of a pass's kernel ("" when the pass is not compiled: its matrix
 // pool, passed as a kernel parameter, would exceed kJitMaxCoef entries).
 constexpr int kJitMaxCoef = 3800;
-std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops, int npool);
+std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops, int npool,
+                            bool batch = false);
 // Kernels for the given pass sources (nullptr for an empty source or a failed compile).
-int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out);
+int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out, const char* name = "vqc_pass");
 // A serialised pass for jit_pass_kernels (stages == nullptr: not a tile pass).
 struct JitPassRef {
   const DevStageF* stages = nullptr;
@@ -160,10 +147,26 @@ struct JitPassRef {
   int npool = 0;
 };
 // Kernels for many passes, looked up by a hash of their structure first.
-int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out);
+// batch: the serving loop's kernels (vqc_pass_batch over an array of TileItems,
+// coefficients from each item's pool) instead of the single-state ones.
+// compile = false: look up only (a structure not compiled yet gives nullptr).
+int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out,
+                     bool batch = false, bool compile = true);
 
+// compiled: an FP32 packed plan with compiled batch kernels (fwd_k / adj_k)
+// when every pass has one already, else the classic plan for the generic
+// kernel; then *to_compile (if given) receives the packed plan whose missing
+// kernels the caller compiles afterwards (serve_compile_plan) for later
+// requests of the same structure.
 int serve_build_plan(int n, int dtype, const std::vector<GateSpec>& fspecs, const std::vector<GateSpec>& rspecs,
-                     const std::vector<std::vector<ParamInfo>>& params, bool want_grad, ReqPlan& rp);
+                     const std::vector<std::vector<ParamInfo>>& params, bool want_grad, bool compiled, ReqPlan& rp,
+                     ReqPlan* to_compile = nullptr);
+void serve_compile_plan(const ReqPlan& packed, bool want_grad);
+// CTAs per request of the compiled batch kernels ks of a plan's passes.
+int serve_jit_gridx(int M, bool adj, const std::vector<const void*>& ks, const SerialPlan& sp, int64_t ntiles,
+                    int device);
+int serve_launch_jit(int M, bool adj, const void* kernel, const TileItem* d_items, int nitems, int gridx,
+                     const PassShape& maxs, cudaStream_t stream);
 int serve_tile_gridx(int dtype, int M, bool adj, const PassShape& maxs, int64_t max_ntiles, int device);
 int serve_launch_tiles(int dtype, int M, bool adj, const TileItem* d_items, int nitems, int gridx,
                        const PassShape& maxs, cudaStream_t stream);
