@@ -104,30 +104,40 @@ __host__ __device__ __forceinline__ uint32_t swz_pair(uint32_t p) {
 constexpr int kPoolFree[5] = {12, 6, 4, 6, 0};
 constexpr int kPoolLane[5] = {6, 3, 2, 3, 0};
 
+// Every free layout stores an imaginary part next to its negation, so conj(U)
+// (CJ: the reverse sweep holds the cotangent conjugated) is U with the two
+// exchanged: a compile-time permutation of the coefficient indices.
+template <bool CJ>
+struct FreeIx {
+  static constexpr int i1 = CJ ? 2 : 1, i2 = CJ ? 1 : 2, i4 = CJ ? 5 : 4, i5 = CJ ? 4 : 5, i7 = CJ ? 8 : 7,
+                       i8 = CJ ? 7 : 8, i10 = CJ ? 11 : 10, i11 = CJ ? 10 : 11;
+};
+
 // Two pairs at once: (A, B) = amplitudes with target bit 0 / 1, both lanes.
-template <int FORM>
+template <int FORM, bool CJ = false>
 __device__ __forceinline__ void free_apply(Pk& A, Pk& B, const u64* c) {
+  using I = FreeIx<CJ>;
   const u64 ar = A.r, ai = A.i, br = B.r, bi = B.i;
   if (FORM == kFormGen) {
-    A.r = fma2(c[0], ar, fma2(c[2], ai, fma2(c[3], br, mul2(c[5], bi))));
-    A.i = fma2(c[0], ai, fma2(c[1], ar, fma2(c[3], bi, mul2(c[4], br))));
-    B.r = fma2(c[6], ar, fma2(c[8], ai, fma2(c[9], br, mul2(c[11], bi))));
-    B.i = fma2(c[6], ai, fma2(c[7], ar, fma2(c[9], bi, mul2(c[10], br))));
+    A.r = fma2(c[0], ar, fma2(c[I::i2], ai, fma2(c[3], br, mul2(c[I::i5], bi))));
+    A.i = fma2(c[0], ai, fma2(c[I::i1], ar, fma2(c[3], bi, mul2(c[I::i4], br))));
+    B.r = fma2(c[6], ar, fma2(c[I::i8], ai, fma2(c[9], br, mul2(c[I::i11], bi))));
+    B.i = fma2(c[6], ai, fma2(c[I::i7], ar, fma2(c[9], bi, mul2(c[I::i10], br))));
   } else if (FORM == kFormRI) {
-    A.r = fma2(c[0], ar, mul2(c[2], bi));
-    A.i = fma2(c[0], ai, mul2(c[1], br));
-    B.r = fma2(c[3], br, mul2(c[5], ai));
-    B.i = fma2(c[3], bi, mul2(c[4], ar));
+    A.r = fma2(c[0], ar, mul2(c[I::i2], bi));
+    A.i = fma2(c[0], ai, mul2(c[I::i1], br));
+    B.r = fma2(c[3], br, mul2(c[I::i5], ai));
+    B.i = fma2(c[3], bi, mul2(c[I::i4], ar));
   } else if (FORM == kFormReal) {
     A.r = fma2(c[0], ar, mul2(c[1], br));
     A.i = fma2(c[0], ai, mul2(c[1], bi));
     B.r = fma2(c[2], ar, mul2(c[3], br));
     B.i = fma2(c[2], ai, mul2(c[3], bi));
   } else if (FORM == kFormDiag) {
-    A.r = fma2(c[0], ar, mul2(c[2], ai));
-    A.i = fma2(c[0], ai, mul2(c[1], ar));
-    B.r = fma2(c[3], br, mul2(c[5], bi));
-    B.i = fma2(c[3], bi, mul2(c[4], br));
+    A.r = fma2(c[0], ar, mul2(c[I::i2], ai));
+    A.i = fma2(c[0], ai, mul2(c[I::i1], ar));
+    B.r = fma2(c[3], br, mul2(c[I::i5], bi));
+    B.i = fma2(c[3], bi, mul2(c[I::i4], br));
   } else {
     const Pk t = A;
     A = B;
@@ -136,31 +146,32 @@ __device__ __forceinline__ void free_apply(Pk& A, Pk& B, const u64* c) {
 }
 
 // One lane of two pairs (the pair of that lane), free layout, scalar.
-template <int FORM, int LANE>
+template <int FORM, int LANE, bool CJ = false>
 __device__ __forceinline__ void scalar_apply(Pk& A, Pk& B, const u64* c) {
+  using I = FreeIx<CJ>;
   const float Ar = LANE ? hi(A.r) : lo(A.r), Ai = LANE ? hi(A.i) : lo(A.i);
   const float Br = LANE ? hi(B.r) : lo(B.r), Bi = LANE ? hi(B.i) : lo(B.i);
   float ar, ai, br, bi;
   if (FORM == kFormGen) {
-    ar = fmaf(lo(c[0]), Ar, fmaf(lo(c[2]), Ai, fmaf(lo(c[3]), Br, lo(c[5]) * Bi)));
-    ai = fmaf(lo(c[0]), Ai, fmaf(lo(c[1]), Ar, fmaf(lo(c[3]), Bi, lo(c[4]) * Br)));
-    br = fmaf(lo(c[6]), Ar, fmaf(lo(c[8]), Ai, fmaf(lo(c[9]), Br, lo(c[11]) * Bi)));
-    bi = fmaf(lo(c[6]), Ai, fmaf(lo(c[7]), Ar, fmaf(lo(c[9]), Bi, lo(c[10]) * Br)));
+    ar = fmaf(lo(c[0]), Ar, fmaf(lo(c[I::i2]), Ai, fmaf(lo(c[3]), Br, lo(c[I::i5]) * Bi)));
+    ai = fmaf(lo(c[0]), Ai, fmaf(lo(c[I::i1]), Ar, fmaf(lo(c[3]), Bi, lo(c[I::i4]) * Br)));
+    br = fmaf(lo(c[6]), Ar, fmaf(lo(c[I::i8]), Ai, fmaf(lo(c[9]), Br, lo(c[I::i11]) * Bi)));
+    bi = fmaf(lo(c[6]), Ai, fmaf(lo(c[I::i7]), Ar, fmaf(lo(c[9]), Bi, lo(c[I::i10]) * Br)));
   } else if (FORM == kFormRI) {
-    ar = fmaf(lo(c[0]), Ar, lo(c[2]) * Bi);
-    ai = fmaf(lo(c[0]), Ai, lo(c[1]) * Br);
-    br = fmaf(lo(c[3]), Br, lo(c[5]) * Ai);
-    bi = fmaf(lo(c[3]), Bi, lo(c[4]) * Ar);
+    ar = fmaf(lo(c[0]), Ar, lo(c[I::i2]) * Bi);
+    ai = fmaf(lo(c[0]), Ai, lo(c[I::i1]) * Br);
+    br = fmaf(lo(c[3]), Br, lo(c[I::i5]) * Ai);
+    bi = fmaf(lo(c[3]), Bi, lo(c[I::i4]) * Ar);
   } else if (FORM == kFormReal) {
     ar = fmaf(lo(c[0]), Ar, lo(c[1]) * Br);
     ai = fmaf(lo(c[0]), Ai, lo(c[1]) * Bi);
     br = fmaf(lo(c[2]), Ar, lo(c[3]) * Br);
     bi = fmaf(lo(c[2]), Ai, lo(c[3]) * Bi);
   } else if (FORM == kFormDiag) {
-    ar = fmaf(lo(c[0]), Ar, lo(c[2]) * Ai);
-    ai = fmaf(lo(c[0]), Ai, lo(c[1]) * Ar);
-    br = fmaf(lo(c[3]), Br, lo(c[5]) * Bi);
-    bi = fmaf(lo(c[3]), Bi, lo(c[4]) * Br);
+    ar = fmaf(lo(c[0]), Ar, lo(c[I::i2]) * Ai);
+    ai = fmaf(lo(c[0]), Ai, lo(c[I::i1]) * Ar);
+    br = fmaf(lo(c[3]), Br, lo(c[I::i5]) * Bi);
+    bi = fmaf(lo(c[3]), Bi, lo(c[I::i4]) * Br);
   } else {
     ar = Br, ai = Bi, br = Ar, bi = Ai;
   }
@@ -171,23 +182,27 @@ __device__ __forceinline__ void scalar_apply(Pk& A, Pk& B, const u64* c) {
   }
 }
 
-// The pair inside one register pair set (target = lane bit), lane layout.
-template <int FORM>
+// The pair inside one register pair set (target = lane bit), lane layout;
+// CJ: conj(U) (the negated imaginary parts exchanged with the plain ones).
+template <int FORM, bool CJ = false>
 __device__ __forceinline__ void lane_apply(Pk& V, const u64* c) {
   const u64 pr = V.r, pi = V.i;
   if (FORM == kFormGen) {
+    constexpr int g2 = CJ ? 3 : 2, g3 = CJ ? 2 : 3, g4 = CJ ? 5 : 4, g5 = CJ ? 4 : 5;
     const u64 qr = swp(pr), qi = swp(pi);
-    V.r = fma2(c[0], pr, fma2(c[1], qr, fma2(c[3], pi, mul2(c[5], qi))));
-    V.i = fma2(c[0], pi, fma2(c[1], qi, fma2(c[2], pr, mul2(c[4], qr))));
+    V.r = fma2(c[0], pr, fma2(c[1], qr, fma2(c[g3], pi, mul2(c[g5], qi))));
+    V.i = fma2(c[0], pi, fma2(c[1], qi, fma2(c[g2], pr, mul2(c[g4], qr))));
   } else if (FORM == kFormRI) {
-    V.r = fma2(c[0], pr, mul2(c[1], swp(pi)));
-    V.i = fma2(c[0], pi, mul2(c[2], swp(pr)));
+    constexpr int r1 = CJ ? 2 : 1, r2 = CJ ? 1 : 2;
+    V.r = fma2(c[0], pr, mul2(c[r1], swp(pi)));
+    V.i = fma2(c[0], pi, mul2(c[r2], swp(pr)));
   } else if (FORM == kFormReal) {
     V.r = fma2(c[0], pr, mul2(c[1], swp(pr)));
     V.i = fma2(c[0], pi, mul2(c[1], swp(pi)));
   } else if (FORM == kFormDiag) {
-    V.r = fma2(c[0], pr, mul2(c[2], pi));
-    V.i = fma2(c[0], pi, mul2(c[1], pr));
+    constexpr int d1 = CJ ? 2 : 1, d2 = CJ ? 1 : 2;
+    V.r = fma2(c[0], pr, mul2(c[d2], pi));
+    V.i = fma2(c[0], pi, mul2(c[d1], pr));
   } else {
     V.r = swp(pr);
     V.i = swp(pi);
@@ -203,7 +218,7 @@ __device__ __forceinline__ void u1_static(Pk (&v)[8], Pk (&w)[8], const u64* c) 
     for (int m = 0; m < 8; ++m) {
       if (CB > 0 && !((m >> (CB - 1)) & 1)) continue;
       lane_apply<FORM>(v[m], c);
-      if (ADJ) lane_apply<FORM>(w[m], c);
+      if (ADJ) lane_apply<FORM, true>(w[m], c);
     }
   } else {
     constexpr int T = TB - 1;
@@ -213,10 +228,10 @@ __device__ __forceinline__ void u1_static(Pk (&v)[8], Pk (&w)[8], const u64* c) 
       if (CB > 0 && !((m0 >> (CB - 1)) & 1)) continue;
       if (CB == 0) {  // lane control: lane 1 only
         scalar_apply<FORM, 1>(v[m0], v[m1], c);
-        if (ADJ) scalar_apply<FORM, 1>(w[m0], w[m1], c);
+        if (ADJ) scalar_apply<FORM, 1, true>(w[m0], w[m1], c);
       } else {
         free_apply<FORM>(v[m0], v[m1], c);
-        if (ADJ) free_apply<FORM>(w[m0], w[m1], c);
+        if (ADJ) free_apply<FORM, true>(w[m0], w[m1], c);
       }
     }
   }
@@ -231,7 +246,7 @@ __device__ __forceinline__ void u1_masked(Pk (&v)[8], Pk (&w)[8], const u64* c, 
     for (int m = 0; m < 8; ++m) {
       if (!((rmask >> (2 * m)) & 1)) continue;
       lane_apply<FORM>(v[m], c);
-      if (ADJ) lane_apply<FORM>(w[m], c);
+      if (ADJ) lane_apply<FORM, true>(w[m], c);
     }
   } else {
     constexpr int T = TB - 1;
@@ -240,110 +255,117 @@ __device__ __forceinline__ void u1_masked(Pk (&v)[8], Pk (&w)[8], const u64* c, 
       const int m0 = ((g >> T) << (T + 1)) | (g & ((1 << T) - 1)), m1 = m0 | (1 << T);
       if ((rmask >> (2 * m0)) & 1) {
         scalar_apply<FORM, 0>(v[m0], v[m1], c);
-        if (ADJ) scalar_apply<FORM, 0>(w[m0], w[m1], c);
+        if (ADJ) scalar_apply<FORM, 0, true>(w[m0], w[m1], c);
       }
       if ((rmask >> (2 * m0 + 1)) & 1) {
         scalar_apply<FORM, 1>(v[m0], v[m1], c);
-        if (ADJ) scalar_apply<FORM, 1>(w[m0], w[m1], c);
+        if (ADJ) scalar_apply<FORM, 1, true>(w[m0], w[m1], c);
       }
     }
   }
 }
 
 // ----------------------------------------------------------------------------- reduced-matrix accumulation
-// A[a][b] += conj(lam_a) psi_b over the op's pairs, after the uncompute.
-// A thread's partials s[8] = (A00r, A00i, A01r, A01i, A10r, A10i, A11r, A11i).
+// A[a][b] += conj(lam_a) psi_b over the op's pairs, after the uncompute.  The
+// reverse sweep holds the cotangent conjugated (M = conj(lam), loaded and
+// stored conjugated at HBM), so A[a][b] = sum M_a psi_b: Re = Mr Pr - Mi Pi,
+// Im = Mr Pi + Mi Pr.  A thread's partials s[8] = (A00r, A00i, A01r, A01i,
+// A10r, A10i, A11r, A11i).
 template <int KIND>
-__device__ __forceinline__ void acc_free(u64 (&a)[8], const Pk& L0, const Pk& L1, const Pk& P0, const Pk& P1) {
-  const u64 n0i = neg2(L0.i), n1i = neg2(L1.i);
+__device__ __forceinline__ void acc_free(u64 (&a)[8], const Pk& M0, const Pk& M1, const Pk& P0, const Pk& P1) {
+  const u64 n0i = neg2(M0.i), n1i = neg2(M1.i);
   if (KIND != kAccOff) {
-    a[0] = fma2(L0.r, P0.r, fma2(L0.i, P0.i, a[0]));
-    a[1] = fma2(L0.r, P0.i, fma2(n0i, P0.r, a[1]));
-    a[6] = fma2(L1.r, P1.r, fma2(L1.i, P1.i, a[6]));
-    a[7] = fma2(L1.r, P1.i, fma2(n1i, P1.r, a[7]));
+    a[0] = fma2(M0.r, P0.r, fma2(n0i, P0.i, a[0]));
+    a[1] = fma2(M0.r, P0.i, fma2(M0.i, P0.r, a[1]));
+    a[6] = fma2(M1.r, P1.r, fma2(n1i, P1.i, a[6]));
+    a[7] = fma2(M1.r, P1.i, fma2(M1.i, P1.r, a[7]));
   }
   if (KIND != kAccDiag) {
-    a[2] = fma2(L0.r, P1.r, fma2(L0.i, P1.i, a[2]));
-    a[3] = fma2(L0.r, P1.i, fma2(n0i, P1.r, a[3]));
-    a[4] = fma2(L1.r, P0.r, fma2(L1.i, P0.i, a[4]));
-    a[5] = fma2(L1.r, P0.i, fma2(n1i, P0.r, a[5]));
+    a[2] = fma2(M0.r, P1.r, fma2(n0i, P1.i, a[2]));
+    a[3] = fma2(M0.r, P1.i, fma2(M0.i, P1.r, a[3]));
+    a[4] = fma2(M1.r, P0.r, fma2(n1i, P0.i, a[4]));
+    a[5] = fma2(M1.r, P0.i, fma2(M1.i, P0.r, a[5]));
   }
 }
 template <int KIND, int LANE>
-__device__ __forceinline__ void acc_scalar(float (&s)[8], const Pk& L0, const Pk& L1, const Pk& P0, const Pk& P1) {
-  const float l0r = LANE ? hi(L0.r) : lo(L0.r), l0i = LANE ? hi(L0.i) : lo(L0.i);
-  const float l1r = LANE ? hi(L1.r) : lo(L1.r), l1i = LANE ? hi(L1.i) : lo(L1.i);
+__device__ __forceinline__ void acc_scalar(float (&s)[8], const Pk& M0, const Pk& M1, const Pk& P0, const Pk& P1) {
+  const float m0r = LANE ? hi(M0.r) : lo(M0.r), m0i = LANE ? hi(M0.i) : lo(M0.i);
+  const float m1r = LANE ? hi(M1.r) : lo(M1.r), m1i = LANE ? hi(M1.i) : lo(M1.i);
   const float p0r = LANE ? hi(P0.r) : lo(P0.r), p0i = LANE ? hi(P0.i) : lo(P0.i);
   const float p1r = LANE ? hi(P1.r) : lo(P1.r), p1i = LANE ? hi(P1.i) : lo(P1.i);
   if (KIND != kAccOff) {
-    s[0] = fmaf(l0r, p0r, fmaf(l0i, p0i, s[0]));
-    s[1] = fmaf(l0r, p0i, fmaf(-l0i, p0r, s[1]));
-    s[6] = fmaf(l1r, p1r, fmaf(l1i, p1i, s[6]));
-    s[7] = fmaf(l1r, p1i, fmaf(-l1i, p1r, s[7]));
+    s[0] = fmaf(m0r, p0r, fmaf(-m0i, p0i, s[0]));
+    s[1] = fmaf(m0r, p0i, fmaf(m0i, p0r, s[1]));
+    s[6] = fmaf(m1r, p1r, fmaf(-m1i, p1i, s[6]));
+    s[7] = fmaf(m1r, p1i, fmaf(m1i, p1r, s[7]));
   }
   if (KIND != kAccDiag) {
-    s[2] = fmaf(l0r, p1r, fmaf(l0i, p1i, s[2]));
-    s[3] = fmaf(l0r, p1i, fmaf(-l0i, p1r, s[3]));
-    s[4] = fmaf(l1r, p0r, fmaf(l1i, p0i, s[4]));
-    s[5] = fmaf(l1r, p0i, fmaf(-l1i, p0r, s[5]));
+    s[2] = fmaf(m0r, p1r, fmaf(-m0i, p1i, s[2]));
+    s[3] = fmaf(m0r, p1i, fmaf(m0i, p1r, s[3]));
+    s[4] = fmaf(m1r, p0r, fmaf(-m1i, p0i, s[4]));
+    s[5] = fmaf(m1r, p0i, fmaf(m1i, p0r, s[5]));
   }
 }
 // lane target: c0 = (A00r, A11r), c1 = (A00i, A11i), c2 = (A01r, A10r), c3 = (A01i, A10i)
 template <int KIND>
-__device__ __forceinline__ void acc_lane(u64 (&c)[4], const Pk& L, const Pk& P) {
-  const u64 ni = neg2(L.i);
+__device__ __forceinline__ void acc_lane(u64 (&c)[4], const Pk& M, const Pk& P) {
+  const u64 ni = neg2(M.i);
   if (KIND != kAccOff) {
-    c[0] = fma2(L.r, P.r, fma2(L.i, P.i, c[0]));
-    c[1] = fma2(L.r, P.i, fma2(ni, P.r, c[1]));
+    c[0] = fma2(M.r, P.r, fma2(ni, P.i, c[0]));
+    c[1] = fma2(M.r, P.i, fma2(M.i, P.r, c[1]));
   }
   if (KIND != kAccDiag) {
     const u64 qr = swp(P.r), qi = swp(P.i);
-    c[2] = fma2(L.r, qr, fma2(L.i, qi, c[2]));
-    c[3] = fma2(L.r, qi, fma2(ni, qr, c[3]));
+    c[2] = fma2(M.r, qr, fma2(ni, qi, c[2]));
+    c[3] = fma2(M.r, qi, fma2(M.i, qr, c[3]));
   }
 }
 // Anti-Hermitian projection (KIND & kAccAH): when every matrix D the op's
 // partials contract with is anti-Hermitian (D = U^dagger dU/dtheta of a
 // unitary family), Re sum_ab D_ab A_ab = -Im D00 s0 - Im D11 s1 + Re D01 s2
 // - Im D01 s3 needs only s = (Im A00, Im A11, Re A01 - Re A10, Im A01 + Im A10):
-// three quarters of the products and half the values to reduce.
+// three quarters of the products and half the values to reduce.  With the
+// conjugated cotangent every one of them is a plain sum of products:
+//   s0 = sum M0r P0i + M0i P0r,  s1 = sum M1r P1i + M1i P1r,
+//   s2 = sum (M0r P1r + M1i P0i) - sum (M0i P1i + M1r P0r),
+//   s3 = sum M0r P1i + M0i P1r + M1r P0i + M1i P0r.
 template <int KIND>
-__device__ __forceinline__ void acch_free(u64 (&a)[5], const Pk& L0, const Pk& L1, const Pk& P0, const Pk& P1) {
-  const u64 n0i = neg2(L0.i), n1i = neg2(L1.i);
+__device__ __forceinline__ void acch_free(u64 (&a)[5], const Pk& M0, const Pk& M1, const Pk& P0, const Pk& P1) {
   if ((KIND & 3) != kAccOff) {
-    a[0] = fma2(L0.r, P0.i, fma2(n0i, P0.r, a[0]));
-    a[1] = fma2(L1.r, P1.i, fma2(n1i, P1.r, a[1]));
+    a[0] = fma2(M0.r, P0.i, fma2(M0.i, P0.r, a[0]));
+    a[1] = fma2(M1.r, P1.i, fma2(M1.i, P1.r, a[1]));
   }
   if ((KIND & 3) != kAccDiag) {
-    a[2] = fma2(L0.r, P1.r, fma2(L0.i, P1.i, a[2]));
-    a[3] = fma2(L1.r, P0.r, fma2(L1.i, P0.i, a[3]));
-    a[4] = fma2(L0.r, P1.i, fma2(n0i, P1.r, fma2(L1.r, P0.i, fma2(n1i, P0.r, a[4]))));
+    a[2] = fma2(M0.r, P1.r, fma2(M1.i, P0.i, a[2]));
+    a[3] = fma2(M0.i, P1.i, fma2(M1.r, P0.r, a[3]));
+    a[4] = fma2(M0.r, P1.i, fma2(M0.i, P1.r, fma2(M1.r, P0.i, fma2(M1.i, P0.r, a[4]))));
   }
 }
 template <int KIND, int LANE>
-__device__ __forceinline__ void acch_scalar(float (&s)[8], const Pk& L0, const Pk& L1, const Pk& P0, const Pk& P1) {
-  const float l0r = LANE ? hi(L0.r) : lo(L0.r), l0i = LANE ? hi(L0.i) : lo(L0.i);
-  const float l1r = LANE ? hi(L1.r) : lo(L1.r), l1i = LANE ? hi(L1.i) : lo(L1.i);
+__device__ __forceinline__ void acch_scalar(float (&s)[8], const Pk& M0, const Pk& M1, const Pk& P0, const Pk& P1) {
+  const float m0r = LANE ? hi(M0.r) : lo(M0.r), m0i = LANE ? hi(M0.i) : lo(M0.i);
+  const float m1r = LANE ? hi(M1.r) : lo(M1.r), m1i = LANE ? hi(M1.i) : lo(M1.i);
   const float p0r = LANE ? hi(P0.r) : lo(P0.r), p0i = LANE ? hi(P0.i) : lo(P0.i);
   const float p1r = LANE ? hi(P1.r) : lo(P1.r), p1i = LANE ? hi(P1.i) : lo(P1.i);
   if ((KIND & 3) != kAccOff) {
-    s[0] = fmaf(l0r, p0i, fmaf(-l0i, p0r, s[0]));
-    s[1] = fmaf(l1r, p1i, fmaf(-l1i, p1r, s[1]));
+    s[0] = fmaf(m0r, p0i, fmaf(m0i, p0r, s[0]));
+    s[1] = fmaf(m1r, p1i, fmaf(m1i, p1r, s[1]));
   }
   if ((KIND & 3) != kAccDiag) {
-    s[2] = fmaf(l0r, p1r, fmaf(l0i, p1i, fmaf(-l1r, p0r, fmaf(-l1i, p0i, s[2]))));
-    s[3] = fmaf(l0r, p1i, fmaf(-l0i, p1r, fmaf(l1r, p0i, fmaf(-l1i, p0r, s[3]))));
+    s[2] = fmaf(m0r, p1r, fmaf(-m0i, p1i, fmaf(-m1r, p0r, fmaf(m1i, p0i, s[2]))));
+    s[3] = fmaf(m0r, p1i, fmaf(m0i, p1r, fmaf(m1r, p0i, fmaf(m1i, p0r, s[3]))));
   }
 }
-// lane target: c0 = (Im A00, Im A11), c1 = (Re A01, Re A10), c2 = (Im A01, Im A10)
+// lane target: c0 = (Im A00, Im A11); (Re A01, Re A10) = c1 - c2 with
+// c1 = Mr Qr, c2 = Mi Qi (Q = the lane-swapped P); c3 = (Im A01, Im A10)
 template <int KIND>
-__device__ __forceinline__ void acch_lane(u64 (&c)[3], const Pk& L, const Pk& P) {
-  const u64 ni = neg2(L.i);
-  if ((KIND & 3) != kAccOff) c[0] = fma2(L.r, P.i, fma2(ni, P.r, c[0]));
+__device__ __forceinline__ void acch_lane(u64 (&c)[4], const Pk& M, const Pk& P) {
+  if ((KIND & 3) != kAccOff) c[0] = fma2(M.r, P.i, fma2(M.i, P.r, c[0]));
   if ((KIND & 3) != kAccDiag) {
     const u64 qr = swp(P.r), qi = swp(P.i);
-    c[1] = fma2(L.r, qr, fma2(L.i, qi, c[1]));
-    c[2] = fma2(L.r, qi, fma2(ni, qr, c[2]));
+    c[1] = fma2(M.r, qr, c[1]);
+    c[2] = fma2(M.i, qi, c[2]);
+    c[3] = fma2(M.r, qi, fma2(M.i, qr, c[3]));
   }
 }
 __device__ __forceinline__ void packh_free(const u64 (&a)[5], float (&s)[8]) {
@@ -352,8 +374,8 @@ __device__ __forceinline__ void packh_free(const u64 (&a)[5], float (&s)[8]) {
   s[2] = (lo(a[2]) + hi(a[2])) - (lo(a[3]) + hi(a[3]));
   s[3] = lo(a[4]) + hi(a[4]);
 }
-__device__ __forceinline__ void packh_lane(const u64 (&c)[3], float (&s)[8]) {
-  s[0] = lo(c[0]), s[1] = hi(c[0]), s[2] = lo(c[1]) - hi(c[1]), s[3] = lo(c[2]) + hi(c[2]);
+__device__ __forceinline__ void packh_lane(const u64 (&c)[4], float (&s)[8]) {
+  s[0] = lo(c[0]), s[1] = hi(c[0]), s[2] = (lo(c[1]) - lo(c[2])) - (hi(c[1]) - hi(c[2])), s[3] = lo(c[3]) + hi(c[3]);
 }
 __device__ __forceinline__ void pack_free(const u64 (&a)[8], float (&s)[8]) {
 #pragma unroll
@@ -411,7 +433,7 @@ __device__ __forceinline__ void flush4(const float (&s)[8], double* sacc, int sl
 template <int TB, int CB, int KIND>
 __device__ __forceinline__ void acc_static(const Pk (&v)[8], const Pk (&w)[8], float (&s8)[8]) {
   if constexpr ((KIND & kAccAH) && TB == 0) {
-    u64 c[3] = {0, 0, 0};
+    u64 c[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       if (CB > 0 && !((m >> (CB - 1)) & 1)) continue;
@@ -465,7 +487,7 @@ __device__ __forceinline__ void acc_static(const Pk (&v)[8], const Pk (&w)[8], f
 template <int TB, int KIND>
 __device__ __forceinline__ void acc_masked(const Pk (&v)[8], const Pk (&w)[8], uint32_t rmask, float (&s8)[8]) {
   if constexpr ((KIND & kAccAH) && TB == 0) {
-    u64 c[3] = {0, 0, 0};
+    u64 c[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int m = 0; m < 8; ++m)
       if ((rmask >> (2 * m)) & 1) acch_lane<KIND>(c, w[m], v[m]);
@@ -583,10 +605,15 @@ __device__ __forceinline__ void u2_op(Pk (&v)[8], Pk (&w)[8], const float2* U, u
 #pragma unroll
       for (int i = 0; i < 4; ++i) x[i] = amp(s, idx[i]);
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        o[r] = ccmul(U[4 * r], x[0]);
+      for (int r = 0; r < 4; ++r) {  // the cotangent (st == 1, held conjugated) with conj(U)
+        const float sg = st ? -1.f : 1.f;
+        const float2 u0 = U[4 * r];
+        o[r] = ccmul(make_float2(u0.x, sg * u0.y), x[0]);
 #pragma unroll
-        for (int cc = 1; cc < 4; ++cc) o[r] = ccfma(U[4 * r + cc], x[cc], o[r]);
+        for (int cc = 1; cc < 4; ++cc) {
+          const float2 u = U[4 * r + cc];
+          o[r] = ccfma(make_float2(u.x, sg * u.y), x[cc], o[r]);
+        }
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i) set_amp(s, idx[i], o[i]);
@@ -628,7 +655,7 @@ __device__ __forceinline__ void diag_op(Pk (&v)[8], Pk (&w)[8], const DevOp* op,
       if (db[i] >= 0) idx |= ((t >> db[i]) & 1u) << i;
     const float2 d = c[idx];
     set_amp(v, j, ccmul(d, amp(v, j)));
-    if (ADJ) set_amp(w, j, ccmul(d, amp(w, j)));
+    if (ADJ) set_amp(w, j, ccmul(make_float2(d.x, -d.y), amp(w, j)));  // the conjugated cotangent
   }
 }
 // Bins of conj(lam) psi over a diagonal op's (at most 2) qubits -> s8.
@@ -649,8 +676,8 @@ __device__ __forceinline__ void accd_op(const Pk (&v)[8], const Pk (&w)[8], cons
 #pragma unroll
     for (int i = 0; i < 2; ++i)
       if (db[i] >= 0) idx |= ((t >> db[i]) & 1u) << i;
-    const float2 l = amp(w, j), p = amp(v, j);
-    const float re = fmaf(l.x, p.x, l.y * p.y), im = fmaf(l.x, p.y, -l.y * p.x);
+    const float2 m = amp(w, j), p = amp(v, j);  // m = conj(lam)
+    const float re = fmaf(m.x, p.x, -m.y * p.y), im = fmaf(m.x, p.y, m.y * p.x);
 #pragma unroll
     for (int b = 0; b < 4; ++b)
       if (idx == (uint32_t)b) {
@@ -758,10 +785,10 @@ __device__ __forceinline__ void stage_load(const TileCtx<M, ADJ>& x, const DevSt
       const float4 t = *reinterpret_cast<const float4*>(x.psi + gi);
       v[m].r = mk(t.x, t.z);
       v[m].i = mk(t.y, t.w);
-      if (ADJ) {
+      if (ADJ) {  // the cotangent is held conjugated
         const float4 u = *reinterpret_cast<const float4*>(x.lam + gi);
         w[m].r = mk(u.x, u.z);
-        w[m].i = mk(u.y, u.w);
+        w[m].i = mk(-u.y, -u.w);
       }
     }
   } else {
@@ -792,8 +819,8 @@ __device__ __forceinline__ void stage_store(const TileCtx<M, ADJ>& x, const DevS
       const int64_t gi = g0 + S->gdep[m];
       if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       *reinterpret_cast<float4*>(x.psi + gi) = make_float4(lo(v[m].r), lo(v[m].i), hi(v[m].r), hi(v[m].i));
-      if (ADJ)
-        *reinterpret_cast<float4*>(x.lam + gi) = make_float4(lo(w[m].r), lo(w[m].i), hi(w[m].r), hi(w[m].i));
+      if (ADJ)  // conjugated back
+        *reinterpret_cast<float4*>(x.lam + gi) = make_float4(lo(w[m].r), -lo(w[m].i), hi(w[m].r), -hi(w[m].i));
     }
   } else {
     const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
@@ -821,10 +848,10 @@ __device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ>& x, const Dev
       const float4 t = *reinterpret_cast<const float4*>(x.psi + gi);
       v[m].r = mk(t.x, t.z);
       v[m].i = mk(t.y, t.w);
-      if (ADJ) {
+      if (ADJ) {  // the cotangent is held conjugated
         const float4 u = *reinterpret_cast<const float4*>(x.lam + gi);
         w[m].r = mk(u.x, u.z);
-        w[m].i = mk(u.y, u.w);
+        w[m].i = mk(-u.y, -u.w);
       }
     }
   } else {
@@ -855,8 +882,8 @@ __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const De
       const int64_t gi = g0 + gdep[m];
       if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       *reinterpret_cast<float4*>(x.psi + gi) = make_float4(lo(v[m].r), lo(v[m].i), hi(v[m].r), hi(v[m].i));
-      if (ADJ)
-        *reinterpret_cast<float4*>(x.lam + gi) = make_float4(lo(w[m].r), lo(w[m].i), hi(w[m].r), hi(w[m].i));
+      if (ADJ)  // conjugated back
+        *reinterpret_cast<float4*>(x.lam + gi) = make_float4(lo(w[m].r), -lo(w[m].i), hi(w[m].r), -hi(w[m].i));
     }
   } else {
     const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
