@@ -11,6 +11,7 @@
 // phase f_x(i) = sum_t c_t i^{|x & z_t|} (-1)^{|(i ^ x) & z_t|}.  All sums are
 // FP64 (also for FP32 states) and reduced in a fixed order.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 
@@ -269,21 +270,37 @@ __global__ void __launch_bounds__(kRedThreads)
 // above gives one phase for all four.  For the XXZ chain each flip-mask group
 // is one window, the diagonal group five.
 constexpr int kWinBits = 6, kWinSize = 1 << kWinBits;
+static bool env_on(const char* name, bool dflt) {
+  const char* v = std::getenv(name);
+  return v && *v ? std::atoi(v) != 0 : dflt;
+}
 constexpr size_t kWinMaxTableBytes = 96 * 1024;
 struct DevGroupW {
   uint64_t x;
   int wbeg, wend;  // windows [wbeg, wend); window wbeg starts at bit 0 when low0
-  int tbeg, tend;  // terms in no window: signs evaluated per partner
+  int tbeg, tend;  // terms in no window: signs evaluated directly
   int low0;
-  int pad;
+  int rlow;  // 1: a term in no window has Z on qubit 0 or 1 (the four partners' phases differ)
 };
 
-template <class R, bool WRITE, bool ACC>
+// Traversal: with thl > 0 the linear quad counter t maps to the quad index
+// k whose bits [0, tlo) are t's lowest bits (coalesced lanes), bits
+// [ths, ths + thl) (the top of the index) its next thl bits, and bits
+// [tlo, ths) the rest: every combination of the top bits is in flight at once,
+// so flip masks on those bits find their partners among the amplitudes being
+// read.  ADD: out accumulates (out += df H psi) instead of being overwritten.
+__device__ __forceinline__ int64_t pauli_trav(int64_t t, int tlo, int ths, int thl) {
+  if (thl == 0) return t;
+  const int64_t lo = t & ((int64_t(1) << tlo) - 1), hi = (t >> tlo) & ((int64_t(1) << thl) - 1);
+  return lo | (hi << ths) | ((t >> (tlo + thl)) << tlo);
+}
+
+template <class R, bool WRITE, bool ACC, bool ADD>
 __global__ void __launch_bounds__(kRedThreads)
     k_pauli_win(const cplx<R>* __restrict__ bra, const cplx<R>* __restrict__ ket, cplx<R>* __restrict__ out,
                 int64_t N, const DevGroupW* __restrict__ groups, int ng, const int* __restrict__ shifts,
                 const cplx<R>* __restrict__ tables, int nw, const DevTerm* __restrict__ terms, int nt, double dfac,
-                Scratch s, double* res) {
+                int tlo, int ths, int thl, Scratch s, double* res) {
   using V = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem[];
   V* stab = reinterpret_cast<V*>(smem);
@@ -301,8 +318,8 @@ __global__ void __launch_bounds__(kRedThreads)
   double acc[2] = {0, 0};
   const V zero = mkc<R>(R(0), R(0));
   const int64_t stride = (int64_t)gridDim.x * blockDim.x, nq4 = N >> 2;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nq4; k += stride) {
-    const int64_t i0 = k << 2;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nq4; t += stride) {
+    const int64_t i0 = pauli_trav(t, tlo, ths, thl) << 2;
     V hv[4];
 #pragma unroll
     for (int a = 0; a < 4; ++a) hv[a] = zero;
@@ -315,7 +332,7 @@ __global__ void __launch_bounds__(kRedThreads)
       int w = g.wbeg;
       V f = zero;
       V W[4];
-      const bool four = g.low0 || g.tbeg < g.tend;
+      const bool four = g.low0 || g.rlow;
       if (g.low0) {
         const V* t = stab + (size_t)w * kWinSize + (jb & (kWinSize - 1));
 #pragma unroll
@@ -334,6 +351,11 @@ __global__ void __launch_bounds__(kRedThreads)
         const uint64_t m = (uint64_t)jb & st[q].z;
         const int hb = (__popc((unsigned)m ^ (unsigned)(m >> 32)) & 1);
         const V cc = st[q].c;
+        if ((st[q].z & 3) == 0) {  // the same phase at the four partners
+          f.x += hb ? -cc.x : cc.x;
+          f.y += hb ? -cc.y : cc.y;
+          continue;
+        }
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
           const bool odd = (hb ^ (__popc((unsigned)(b & st[q].z)) & 1)) != 0;
@@ -361,12 +383,21 @@ __global__ void __launch_bounds__(kRedThreads)
     }
     if (WRITE) {
       const R df = (R)dfac;  // 1 or 2
+      V o[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) o[a] = mkc<R>(df * hv[a].x, df * hv[a].y);
+      if (ADD) {
+        V prev[4];
+        load4<R>(out + i0, prev);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) o[a].x += prev[a].x, o[a].y += prev[a].y;
+      }
       if constexpr (sizeof(R) == 4) {
-        *reinterpret_cast<float4*>(out + i0) = make_float4(df * hv[0].x, df * hv[0].y, df * hv[1].x, df * hv[1].y);
-        *reinterpret_cast<float4*>(out + i0 + 2) = make_float4(df * hv[2].x, df * hv[2].y, df * hv[3].x, df * hv[3].y);
+        *reinterpret_cast<float4*>(out + i0) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+        *reinterpret_cast<float4*>(out + i0 + 2) = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
       } else {
 #pragma unroll
-        for (int a = 0; a < 4; ++a) out[i0 + a] = mkc<R>(df * hv[a].x, df * hv[a].y);
+        for (int a = 0; a < 4; ++a) out[i0 + a] = o[a];
       }
     }
     if (ACC) {
@@ -381,6 +412,11 @@ __global__ void __launch_bounds__(kRedThreads)
     }
   }
   if (ACC) grid_reduce<2>(acc, s, res);
+}
+
+// Adds the second launch's sums (res[2..3]) to the first's (res[0..1]).
+__global__ void k_add_pair(double* res) {
+  if (threadIdx.x < 2) res[threadIdx.x] += res[2 + threadIdx.x];
 }
 
 // Window tables of a prepared operator (terms grouped by flip mask; the
@@ -401,16 +437,15 @@ static bool build_windows(const std::vector<DevGroup>& groups, const std::vector
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return lo_of(a) < lo_of(b); });
     struct Win {
       int s;
-      std::vector<cd> tab;
+      std::vector<int> ts;
     };
     std::vector<Win> wins;
     cd c0(0);
     std::vector<DevTerm> rest;
     for (int t : idx) {
       const uint64_t z = terms[t].z;
-      const cd c(terms[t].c.x, terms[t].c.y);
       if (!z) {
-        c0 += c;
+        c0 += cd(terms[t].c.x, terms[t].c.y);
         continue;
       }
       const int lo = __builtin_ctzll(z), hi = 63 - __builtin_clzll(z);
@@ -427,30 +462,61 @@ static bool build_windows(const std::vector<DevGroup>& groups, const std::vector
           rest.push_back(terms[t]);
           continue;
         }
-        wins.push_back(Win{sh, std::vector<cd>(kWinSize, cd(0))});
+        wins.push_back(Win{sh, {}});
         w = &wins.back();
       }
-      const uint64_t zl = z >> w->s;
-      for (int u = 0; u < kWinSize; ++u) w->tab[u] += (__builtin_popcountll((uint64_t)u & zl) & 1) ? -c : c;
+      w->ts.push_back(t);
     }
-    if (c0 != cd(0)) {
-      if (wins.empty()) wins.push_back(Win{2, std::vector<cd>(kWinSize, cd(0))});
-      for (cd& v : wins[0].tab) v += c0;
+    // a table pays for its lookup only when it folds several terms: windows of
+    // one or two terms are evaluated term by term (one parity each)
+    std::vector<Win> keep;
+    for (Win& w : wins) {
+      if ((int)w.ts.size() >= 3) {
+        keep.push_back(std::move(w));
+      } else {
+        for (int t : w.ts) rest.push_back(terms[t]);
+      }
     }
+    wins.swap(keep);
+    if (c0 != cd(0) && wins.empty()) {
+      DevTerm ct{};
+      ct.z = 0;
+      ct.c = make_double2(c0.real(), c0.imag());
+      ct.d = ct.c;
+      rest.push_back(ct);
+      c0 = cd(0);
+    }
+    std::vector<std::vector<cd>> tabs;
+    for (const Win& w : wins) {
+      std::vector<cd> tab(kWinSize, cd(0));
+      for (int t : w.ts) {
+        const cd c(terms[t].c.x, terms[t].c.y);
+        const uint64_t zl = terms[t].z >> w.s;
+        for (int u = 0; u < kWinSize; ++u) tab[u] += (__builtin_popcountll((uint64_t)u & zl) & 1) ? -c : c;
+      }
+      tabs.push_back(std::move(tab));
+    }
+    if (c0 != cd(0))
+      for (cd& v : tabs[0]) v += c0;
     // the window at bit 0 (if any) first
-    std::stable_sort(wins.begin(), wins.end(), [](const Win& a, const Win& b) { return (a.s == 0) > (b.s == 0); });
+    std::vector<int> order(wins.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return (wins[a].s == 0) > (wins[b].s == 0); });
     DevGroupW d{};
     d.x = g.x;
     d.wbeg = (int)pw.shifts.size();
-    for (const Win& w : wins) {
-      pw.shifts.push_back(w.s);
-      pw.tables.insert(pw.tables.end(), w.tab.begin(), w.tab.end());
+    for (int i : order) {
+      pw.shifts.push_back(wins[i].s);
+      pw.tables.insert(pw.tables.end(), tabs[i].begin(), tabs[i].end());
     }
     d.wend = (int)pw.shifts.size();
-    d.low0 = !wins.empty() && wins[0].s == 0;
+    d.low0 = !wins.empty() && wins[order[0]].s == 0;
     d.tbeg = (int)pw.rest.size();
     pw.rest.insert(pw.rest.end(), rest.begin(), rest.end());
     d.tend = (int)pw.rest.size();
+    d.rlow = 0;
+    for (const DevTerm& t : rest)
+      if (t.z & 3) d.rlow = 1;
     pw.groups.push_back(d);
   }
   return pw.tables.size() * amp_bytes <= kWinMaxTableBytes;
@@ -538,6 +604,38 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
     }
     PauliWin pw;
     const bool win = quad && !sep && build_windows(p.groups, p.terms, h->amp_bytes(), pw);
+    // Groups whose flip masks reach beyond the amplitudes one wave of the grid
+    // covers (the XXZ chain's top pairs on a state larger than L2) run in a
+    // second launch whose traversal puts the top bits in the fast dimension, so
+    // their partner reads hit amplitudes read at the same time, not DRAM again.
+    const int grid = reduction_grid(h->device, h->size());
+    int nlow = (int)pw.groups.size(), tlo = 0, ths = 0, thl = 0;
+    if (win && h->nq >= 20 && env_on("VQC_PAULI_SPLIT", true)) {
+      const int nq4 = h->nq - 2, tlo_ = 5;
+      int wave = 0;
+      while ((int64_t(2) << wave) <= (int64_t)grid * kRedThreads) ++wave;  // quad bits one wave covers
+      std::stable_partition(pw.groups.begin(), pw.groups.end(), [&](const DevGroupW& g) {
+        return (g.x >> 2) < (uint64_t(1) << wave);
+      });
+      uint64_t hx = 0;
+      nlow = 0;
+      for (const DevGroupW& g : pw.groups) {
+        if ((g.x >> 2) < (uint64_t(1) << wave))
+          ++nlow;
+        else
+          hx |= g.x >> 2;
+      }
+      if (hx) {
+        const int lowbit = __builtin_ctzll(hx);
+        if (lowbit >= tlo_ && nq4 - lowbit + tlo_ <= wave) {
+          tlo = tlo_;
+          ths = lowbit;
+          thl = nq4 - lowbit;
+        } else {
+          nlow = (int)pw.groups.size();  // no traversal fits: one launch
+        }
+      }
+    }
     std::vector<DevGroup4> g4;
     if (quad && !win) {
       std::vector<DevTerm> sorted;
@@ -588,7 +686,6 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
     const int nw = (int)pw.shifts.size();
     const size_t smem = win ? wtb + gb + shb + pw.rest.size() * (amp == 8 ? sizeof(PTerm<float>) : sizeof(PTerm<double>))
                             : gb + tb;
-    const int grid = reduction_grid(h->device, h->size());
     // a later chunk accumulates onto `out`: run it into a workspace and add
     void* target = out;
     if (write && !first) {  // the third workspace is never an operand of this call
@@ -601,13 +698,31 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
 #define VQC_PAULI_LAUNCH(R)                                                                                      \
   do {                                                                                                           \
     if (win) {                                                                                                   \
-      auto kfun = write ? (acc ? k_pauli_win<R, true, true> : k_pauli_win<R, true, false>)                       \
-                        : k_pauli_win<R, false, true>;                                                           \
-      if (smem > 48 * 1024) VQC_CK(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-      kfun<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,   \
-                                                    h->size(), (const DevGroupW*)(ob + wtb), ng,                 \
-                                                    (const int*)(ob + wtb + gb), (const cplx<R>*)ob, nw, dt, nt, \
-                                                    hermitian_part ? 2.0 : 1.0, h->scr, h->scr.result);          \
+      const DevGroupW* gw = (const DevGroupW*)(ob + wtb);                                                        \
+      const int nhigh = (int)pw.groups.size() - nlow;                                                            \
+      auto k1 = write ? (acc ? k_pauli_win<R, true, true, false> : k_pauli_win<R, true, false, false>)           \
+                      : k_pauli_win<R, false, true, false>;                                                      \
+      auto k2 = write ? (acc ? k_pauli_win<R, true, true, true> : k_pauli_win<R, true, false, true>)             \
+                      : k_pauli_win<R, false, true, true>;                                                       \
+      if (smem > 48 * 1024) {                                                                                    \
+        VQC_CK(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));                \
+        VQC_CK(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));                \
+      }                                                                                                          \
+      k1<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,     \
+                                                  h->size(), gw, nlow, (const int*)(ob + wtb + gb),              \
+                                                  (const cplx<R>*)ob, nw, dt, nt, hermitian_part ? 2.0 : 1.0,   \
+                                                  0, 0, 0, h->scr, h->scr.result);                               \
+      if (nhigh > 0) {                                                                                           \
+        VQC_CK(cudaGetLastError());                                                                              \
+        k2<<<grid, kRedThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)target,   \
+                                                    h->size(), gw + nlow, nhigh, (const int*)(ob + wtb + gb),    \
+                                                    (const cplx<R>*)ob, nw, dt, nt, hermitian_part ? 2.0 : 1.0, \
+                                                    tlo, ths, thl, h->scr, h->scr.result + 2);                   \
+        if (acc) {                                                                                               \
+          VQC_CK(cudaGetLastError());                                                                            \
+          k_add_pair<<<1, 32, 0, h->stream>>>(h->scr.result);                                                    \
+        }                                                                                                        \
+      }                                                                                                          \
     } else if (quad) {                                                                                           \
       auto kfun = write ? (acc ? (sep ? k_pauli4<R, true, true, true> : k_pauli4<R, true, true, false>)          \
                                : (sep ? k_pauli4<R, true, false, true> : k_pauli4<R, true, false, false>))       \
