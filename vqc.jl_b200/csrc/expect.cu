@@ -604,13 +604,16 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
     }
     PauliWin pw;
     const bool win = quad && !sep && build_windows(p.groups, p.terms, h->amp_bytes(), pw);
-    // Groups whose flip masks reach beyond the amplitudes one wave of the grid
-    // covers (the XXZ chain's top pairs on a state larger than L2) run in a
-    // second launch whose traversal puts the top bits in the fast dimension, so
-    // their partner reads hit amplitudes read at the same time, not DRAM again.
+    // VQC_PAULI_SPLIT=1: groups whose flip masks reach beyond the amplitudes one
+    // wave of the grid covers (the XXZ chain's top pairs on a state larger than
+    // L2) run in a second launch whose traversal puts the top bits in the fast
+    // dimension, so their partner reads hit amplitudes read at the same time.
+    // It reads 2.76 GB instead of 3.69 GB at 2^26 FP32 amplitudes but takes
+    // longer on B200 (1.70 against 1.62 ms: the first launch is issue-bound),
+    // so one launch is the default.
     const int grid = reduction_grid(h->device, h->size());
     int nlow = (int)pw.groups.size(), tlo = 0, ths = 0, thl = 0;
-    if (win && h->nq >= 20 && env_on("VQC_PAULI_SPLIT", true)) {
+    if (win && h->nq >= 20 && env_on("VQC_PAULI_SPLIT", false)) {
       const int nq4 = h->nq - 2, tlo_ = 5;
       int wave = 0;
       while ((int64_t(2) << wave) <= (int64_t)grid * kRedThreads) ++wave;  // quad bits one wave covers

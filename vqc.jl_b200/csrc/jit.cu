@@ -293,6 +293,11 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
 
 // Kernels for `srcs` (nullptr where unavailable): cached ones at once, the
 // rest compiled in parallel, then loaded.
+namespace {
+thread_local int t_thread_cap = 0;
+}
+void jit_set_thread_cap(int n) { t_thread_cap = n < 0 ? 0 : n; }
+
 int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out, const char* name) {
   out.assign(srcs.size(), nullptr);
   if (!jit_available()) return VQC_OK;
@@ -315,7 +320,8 @@ int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& 
     std::vector<std::vector<char>> bins(todo.size());
     std::vector<std::string> logs(todo.size());
     std::vector<char> ok(todo.size(), 0);
-    const int nthr = std::max(1, std::min<int>((int)todo.size(), (int)std::thread::hardware_concurrency()));
+    const int hw = std::max(1, (int)std::thread::hardware_concurrency());
+    const int nthr = std::max(1, std::min<int>((int)todo.size(), t_thread_cap > 0 ? std::min(t_thread_cap, hw) : hw));
     std::vector<std::thread> pool;
     std::mutex qm;
     size_t next = 0;

@@ -11,8 +11,10 @@
 //      Pauli pass (energy, and the cotangent (H + H^dagger) psi), a reverse
 //      pass -- and launch the steps of a kind together (a 2-D grid: request x
 //      tiles): FP32 tile passes grouped by pass structure, one launch of that
-//      structure's compiled kernel per group (the planner threads compile each
-//      structure once; requests of one qubit count share most structures),
+//      structure's compiled kernel per group (a background compiler thread,
+//      with a few host cores, compiles each structure once after its first
+//      request has been planned; requests of one qubit count share most
+//      structures; until then they run on the generic kernel),
 //      the others on the generic tile kernel in one launch per tile size;
 //   3. wait for the launches, retire finished requests (results to the host,
 //      memory back to the budget) and loop.
@@ -39,6 +41,7 @@
 namespace vqc {
 
 int launch_grid(int device, int64_t items, int threads, int per_sm);
+constexpr size_t kCompileQueue = 64;  // packed plans waiting for the compiler thread
 
 template <class R>
 __global__ void k_zero_state(cplx<R>* v, int64_t N) {
@@ -108,6 +111,12 @@ struct vqc_server_s {
   std::map<int64_t, std::shared_ptr<vqc::Request>> all;
   std::vector<std::thread> planners;
   std::thread worker;
+  // packed plans whose kernels the compiler thread builds (bounded: a plan
+  // that finds the queue full is dropped; a later request of its structure
+  // queues it again)
+  std::deque<vqc::ReqPlan> to_build;
+  std::condition_variable cv_build;
+  std::thread compiler;
   bool stop = false;
   int64_t next_ticket = 0;
   std::multimap<size_t, double*> pinned_free;  // pinned result buffers by size
@@ -226,9 +235,33 @@ static void planner_main(vqc_server_s* s) {
         s->cv_ready.notify_all();
       }
     }
-    // the request is on its way; compile its structure for the next ones
-    // (other planner threads meanwhile plan other requests)
-    if (!compile_later.fwd.locs.empty()) serve_compile_plan(compile_later, !compile_later.adj.locs.empty());
+    // the request is on its way; its structure is compiled for the next ones
+    // by the compiler thread, so planning never waits for a compile
+    if (!compile_later.fwd.locs.empty()) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->to_build.size() < kCompileQueue) {
+        s->to_build.push_back(std::move(compile_later));
+        s->cv_build.notify_one();
+      }
+    }
+  }
+}
+
+// Compiles queued structures with at most a quarter of the host cores (at
+// least one), so the planners and the GPU worker are not starved meanwhile.
+static void compiler_main(vqc_server_s* s) {
+  cudaSetDevice(s->device);  // kernels are loaded into the server's device context
+  jit_set_thread_cap(std::max(1u, std::thread::hardware_concurrency() / 4));
+  while (true) {
+    ReqPlan p;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_build.wait(lk, [&] { return s->stop || !s->to_build.empty(); });
+      if (s->stop) return;
+      p = std::move(s->to_build.front());
+      s->to_build.pop_front();
+    }
+    serve_compile_plan(p, !p.adj.locs.empty());
   }
 }
 
@@ -584,6 +617,7 @@ int vqc_serve_open(int device, int dtype, size_t memory_bytes, int max_active, i
   const int np = std::max(1, std::min(planner_threads, 16));
   for (int i = 0; i < np; ++i) s->planners.emplace_back(planner_main, s);
   s->worker = std::thread(worker_main, s);
+  s->compiler = std::thread(compiler_main, s);
   *out = s;
   return VQC_OK;
 }
@@ -735,9 +769,11 @@ int vqc_serve_close(vqc_server s) {
     s->stop = true;
     s->cv_plan.notify_all();
     s->cv_ready.notify_all();
+    s->cv_build.notify_all();
   }
   for (auto& t : s->planners) t.join();
   if (s->worker.joinable()) s->worker.join();
+  if (s->compiler.joinable()) s->compiler.join();  // (finishes the compile in progress)
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->stream);
   for (auto& r : s->active) {

@@ -137,6 +137,10 @@ size_t jit_extra_smem(bool adj, int M);
 constexpr int kJitMaxCoef = 3800;
 std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops, int npool,
                             bool batch = false);
+// Compiler threads jit_kernels may start from the calling thread (0: one per
+// host core).  A background compiler sets a few so the threads that plan and
+// launch keep their cores.
+void jit_set_thread_cap(int n);
 // Kernels for the given pass sources (nullptr for an empty source or a failed compile).
 int jit_kernels(const std::vector<std::string>& srcs, std::vector<const void*>& out, const char* name = "vqc_pass");
 // A serialised pass for jit_pass_kernels (stages == nullptr: not a tile pass).
