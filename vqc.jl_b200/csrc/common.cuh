@@ -211,11 +211,11 @@ namespace vqc {
 
 // Block sum of NACC per-thread doubles, then a last-block sum over the grid's
 // block partials in block order.  Deterministic for a fixed grid size.
-// out[i] (device memory) receives the grid total of acc[i].  All threads of the
-// block must call it.
-template <int NACC>
+// out[i] (device memory) receives the grid total of acc[i].  All NT threads
+// of the block (NT = its block size) must call it.
+template <int NACC, int NT = kRedThreads>
 __device__ __forceinline__ void grid_reduce(double (&acc)[NACC], const Scratch& s, double* out) {
-  __shared__ double sm[kRedThreads / 32][NACC];
+  __shared__ double sm[NT / 32][NACC];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -229,7 +229,7 @@ __device__ __forceinline__ void grid_reduce(double (&acc)[NACC], const Scratch& 
   if (threadIdx.x < NACC) {
     double v = 0;
 #pragma unroll
-    for (int w = 0; w < kRedThreads / 32; ++w) v += sm[w][threadIdx.x];
+    for (int w = 0; w < NT / 32; ++w) v += sm[w][threadIdx.x];
     s.partials[(size_t)blockIdx.x * kMaxAcc + threadIdx.x] = v;
   }
   __threadfence();
@@ -240,7 +240,7 @@ __device__ __forceinline__ void grid_reduce(double (&acc)[NACC], const Scratch& 
   __threadfence();
   for (int i = 0; i < NACC; ++i) {
     double v = 0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += kRedThreads)
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += NT)
       v += __ldcg(&s.partials[(size_t)b * kMaxAcc + i]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -249,7 +249,7 @@ __device__ __forceinline__ void grid_reduce(double (&acc)[NACC], const Scratch& 
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0;
-      for (int w = 0; w < kRedThreads / 32; ++w) t += sm[w][0];
+      for (int w = 0; w < NT / 32; ++w) t += sm[w][0];
       out[i] = t;
     }
   }

@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <sstream>
 
 #include "engine.h"
 #include "subspace.cuh"
@@ -419,6 +420,290 @@ __global__ void k_add_pair(double* res) {
   if (threadIdx.x < 2) res[threadIdx.x] += res[2 + threadIdx.x];
 }
 
+// ----------------------------------------------------------------------------- tile passes
+// Pauli sums on states far larger than L2.  One pass streams the state once
+// in tiles of 2^M amplitudes over a chosen set of M qubits (the lowest CLOW
+// qubits always among them: 128-byte runs), staged in shared memory; a group
+// whose flip mask lies inside the tile's qubits reads its partners there
+// instead of from DRAM.  The groups are cut into passes on the host (a first
+// pass over the lowest M qubits, then passes over the high qubits that the
+// remaining flip masks use); a group no pass covers reads its partners from
+// global memory.  Later passes add into the written output (ADD).  REAL: every
+// phase of the operator is real (real Pauli-sum coefficients with an even
+// number of Y per term), so a phase times an amplitude takes two FMAs.
+constexpr int kPTThreads = 512;
+constexpr int kPTHiBits = 9;  // tile bits above the always-resident low qubits
+template <class R>
+struct PTCfg;
+template <>
+struct PTCfg<float> {
+  static constexpr int M = 13, CLOW = 4;  // 64 KiB tile
+};
+template <>
+struct PTCfg<double> {
+  static constexpr int M = 12, CLOW = 3;  // 64 KiB tile
+};
+struct DevPTPass {
+  uint64_t nontile_mask;  // global qubits enumerated by the tile counter
+  int64_t ntiles;
+};
+
+// Shared-memory layout of a tile pass (host and device compute it alike).
+template <class R>
+struct PTLayout {
+  size_t stab, st, sg, shi, sxt, ssh, total;
+  __host__ __device__ PTLayout(int nw, int nt, int ng) {
+    constexpr size_t V = sizeof(cplx<R>);
+    stab = V << PTCfg<R>::M;
+    st = stab + (size_t)nw * kWinSize * V;
+    sg = (st + sizeof(PTerm<R>) * (size_t)nt + 15) & ~size_t(15);
+    shi = sg + sizeof(DevGroupW) * (size_t)ng;
+    sxt = shi + sizeof(int64_t) * (size_t(1) << kPTHiBits);
+    ssh = sxt + sizeof(int) * (size_t)ng;
+    total = (ssh + sizeof(int) * (size_t)nw + 15) & ~size_t(15);
+  }
+};
+
+// Four amplitudes of a tile quad (16-byte aligned) from / to shared memory.
+template <class V>
+__device__ __forceinline__ void tile_ld4(const V* t, V (&kv)[4]) {
+  if constexpr (sizeof(V) == 8) {
+    const float4 a = *reinterpret_cast<const float4*>(t), b = *reinterpret_cast<const float4*>(t + 2);
+    kv[0] = make_float2(a.x, a.y), kv[1] = make_float2(a.z, a.w);
+    kv[2] = make_float2(b.x, b.y), kv[3] = make_float2(b.z, b.w);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) kv[a] = t[a];
+  }
+}
+template <class V>
+__device__ __forceinline__ void tile_st4(V* t, const V (&kv)[4]) {
+  if constexpr (sizeof(V) == 8) {
+    *reinterpret_cast<float4*>(t) = make_float4(kv[0].x, kv[0].y, kv[1].x, kv[1].y);
+    *reinterpret_cast<float4*>(t + 2) = make_float4(kv[2].x, kv[2].y, kv[3].x, kv[3].y);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) t[a] = kv[a];
+  }
+}
+
+// hv += W[b] kv[b] over the four partners b = a ^ AX, real phases (in .x).
+template <int AX, class V>
+__device__ __forceinline__ void pauli4_add_re(V (&hv)[4], const V (&W)[4], const V (&kv)[4]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    hv[a].x = fma(W[a ^ AX].x, kv[a ^ AX].x, hv[a].x);
+    hv[a].y = fma(W[a ^ AX].x, kv[a ^ AX].y, hv[a].y);
+  }
+}
+template <int AX, class V, class S>
+__device__ __forceinline__ void pauli4_add1_re(V (&hv)[4], S f, const V (&kv)[4]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    hv[a].x = fma(f, kv[a ^ AX].x, hv[a].x);
+    hv[a].y = fma(f, kv[a ^ AX].y, hv[a].y);
+  }
+}
+
+template <class R, bool WRITE, bool ACC, bool ADD, bool REAL>
+__global__ void __launch_bounds__(kPTThreads, 2)
+    k_pauli_tile(const cplx<R>* __restrict__ bra, const cplx<R>* __restrict__ ket, cplx<R>* __restrict__ out,
+                 int64_t N, const DevPTPass pass, const DevGroupW* __restrict__ groups, const int* __restrict__ gxt,
+                 int ng, const int64_t* __restrict__ hioff, const int* __restrict__ shifts,
+                 const cplx<R>* __restrict__ tables, int nw, const DevTerm* __restrict__ terms, int nt, double dfac,
+                 Scratch s, double* res) {
+  using V = cplx<R>;
+  constexpr int M = PTCfg<R>::M, CLOW = PTCfg<R>::CLOW, T = 1 << M, QPT = (T >> 2) / kPTThreads;
+  static_assert(M - CLOW == kPTHiBits, "tile layout");
+  extern __shared__ __align__(16) unsigned char smem[];
+  const PTLayout<R> L(nw, nt, ng);
+  V* tile = reinterpret_cast<V*>(smem);
+  V* stab = reinterpret_cast<V*>(smem + L.stab);
+  PTerm<R>* st = reinterpret_cast<PTerm<R>*>(smem + L.st);
+  DevGroupW* sg = reinterpret_cast<DevGroupW*>(smem + L.sg);
+  int64_t* shi = reinterpret_cast<int64_t*>(smem + L.shi);
+  int* sxt = reinterpret_cast<int*>(smem + L.sxt);
+  int* ssh = reinterpret_cast<int*>(smem + L.ssh);
+  __shared__ uint64_t s_base, s_inc;
+  for (int i = threadIdx.x; i < nw * kWinSize; i += kPTThreads) stab[i] = tables[i];
+  for (int i = threadIdx.x; i < nt; i += kPTThreads) {
+    const DevTerm t = terms[i];
+    st[i] = PTerm<R>{t.z, mkc<R>((R)t.c.x, (R)t.c.y), mkc<R>((R)t.c.x, (R)t.c.y)};
+  }
+  for (int i = threadIdx.x; i < ng; i += kPTThreads) sg[i] = groups[i], sxt[i] = gxt[i];
+  for (int i = threadIdx.x; i < (1 << kPTHiBits); i += kPTThreads) shi[i] = hioff[i];
+  for (int i = threadIdx.x; i < nw; i += kPTThreads) ssh[i] = shifts[i];
+  if (threadIdx.x == 0) {
+    // the first tile's base (tile index blockIdx.x spread over the non-tile
+    // qubits) and the increment for gridDim.x tiles
+    uint64_t mm = pass.nontile_mask, b0 = 0, inc = 0;
+    uint64_t t = blockIdx.x, g = gridDim.x;
+    while (mm) {
+      const uint64_t low = mm & (~mm + 1);
+      if (t & 1) b0 |= low;
+      if (g & 1) inc |= low;
+      t >>= 1;
+      g >>= 1;
+      mm ^= low;
+    }
+    s_base = b0;
+    s_inc = inc;
+  }
+  __syncthreads();
+  const uint64_t ntm = pass.nontile_mask, inc = s_inc;
+  uint64_t base = s_base;
+  const V zero = mkc<R>(R(0), R(0));
+  double acc[2] = {0, 0};
+  for (int64_t tl = blockIdx.x; tl < pass.ntiles; tl += gridDim.x) {
+    // the thread's quads: tile quads threadIdx.x + k * kPTThreads
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      const int u = (threadIdx.x + k * kPTThreads) << 2;
+      const int64_t gqk = (int64_t)base + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));
+      V kv[4];
+      if (!VQC_DCHECK(gqk + 3, N)) continue;
+      load4<R>(ket + gqk, kv);
+      tile_st4(tile + u, kv);
+    }
+    __syncthreads();
+    // one quad at a time (four accumulators: the group loop's registers stay few)
+#pragma unroll 1
+    for (int k = 0; k < QPT; ++k) {
+      const int u = (threadIdx.x + k * kPTThreads) << 2;
+      const int64_t gqk = (int64_t)base + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));
+      if (!VQC_DCHECK(gqk + 3, N)) continue;
+      V hv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) hv[a] = zero;
+      for (int gi = 0; gi < ng; ++gi) {
+        const DevGroupW g = sg[gi];
+        const int xt = sxt[gi];
+        const int64_t jb = gqk ^ (int64_t)(g.x & ~3ull);
+        V kv[4];
+        if (xt >= 0) {
+          const int ub = (u ^ xt) & ~3;
+          if (!VQC_DCHECK(ub + 3, T)) continue;
+          tile_ld4(tile + ub, kv);
+        } else {
+          if (!VQC_DCHECK(jb + 3, N)) continue;
+          load4<R>(ket + jb, kv);
+        }
+        int w = g.wbeg;
+        V f = zero, W[4];
+        if (g.low0) {
+          const V* t = stab + (size_t)w * kWinSize + (jb & (kWinSize - 1));
+#pragma unroll
+          for (int b = 0; b < 4; ++b) W[b] = t[b];
+          ++w;
+        } else {
+#pragma unroll
+          for (int b = 0; b < 4; ++b) W[b] = zero;
+        }
+        for (; w < g.wend; ++w) {
+          const V t = stab[(size_t)w * kWinSize + ((jb >> ssh[w]) & (kWinSize - 1))];
+          f.x += t.x;
+          if (!REAL) f.y += t.y;
+        }
+        for (int q = g.tbeg; q < g.tend; ++q) {
+          const uint64_t m = (uint64_t)jb & st[q].z;
+          const int hb = (__popc((unsigned)m ^ (unsigned)(m >> 32)) & 1);
+          const V cc = st[q].c;
+          if ((st[q].z & 3) == 0) {
+            f.x += hb ? -cc.x : cc.x;
+            if (!REAL) f.y += hb ? -cc.y : cc.y;
+            continue;
+          }
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const bool odd = (hb ^ (__popc((unsigned)(b & st[q].z)) & 1)) != 0;
+            W[b].x += odd ? -cc.x : cc.x;
+            if (!REAL) W[b].y += odd ? -cc.y : cc.y;
+          }
+        }
+        const int ax = (int)(g.x & 3);
+        if (g.low0 || g.rlow) {
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            W[b].x += f.x;
+            if (!REAL) W[b].y += f.y;
+          }
+          if (REAL) {
+            switch (ax) {
+              case 0: pauli4_add_re<0>(hv, W, kv); break;
+              case 1: pauli4_add_re<1>(hv, W, kv); break;
+              case 2: pauli4_add_re<2>(hv, W, kv); break;
+              default: pauli4_add_re<3>(hv, W, kv); break;
+            }
+          } else {
+            switch (ax) {
+              case 0: pauli4_add<0>(hv, W, kv); break;
+              case 1: pauli4_add<1>(hv, W, kv); break;
+              case 2: pauli4_add<2>(hv, W, kv); break;
+              default: pauli4_add<3>(hv, W, kv); break;
+            }
+          }
+        } else if (REAL) {
+          switch (ax) {
+            case 0: pauli4_add1_re<0>(hv, f.x, kv); break;
+            case 1: pauli4_add1_re<1>(hv, f.x, kv); break;
+            case 2: pauli4_add1_re<2>(hv, f.x, kv); break;
+            default: pauli4_add1_re<3>(hv, f.x, kv); break;
+          }
+        } else {
+          switch (ax) {
+            case 0: pauli4_add1<0>(hv, f, kv); break;
+            case 1: pauli4_add1<1>(hv, f, kv); break;
+            case 2: pauli4_add1<2>(hv, f, kv); break;
+            default: pauli4_add1<3>(hv, f, kv); break;
+          }
+        }
+      }
+      if (WRITE) {
+        const R df = (R)dfac;  // 1 or 2
+        V o[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) o[a] = mkc<R>(df * hv[a].x, df * hv[a].y);
+        if (ADD) {
+          V prev[4];
+          load4<R>(out + gqk, prev);
+#pragma unroll
+          for (int a = 0; a < 4; ++a) o[a].x += prev[a].x, o[a].y += prev[a].y;
+        }
+        if constexpr (sizeof(R) == 4) {
+          *reinterpret_cast<float4*>(out + gqk) = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+          *reinterpret_cast<float4*>(out + gqk + 2) = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
+        } else {
+#pragma unroll
+          for (int a = 0; a < 4; ++a) out[gqk + a] = o[a];
+        }
+      }
+      if (ACC) {
+        V b[4];
+        if (bra == ket) {
+          tile_ld4(tile + u, b);
+        } else {
+          load4<R>(bra + gqk, b);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const double2 bb = to_d2(b[a]), hh = to_d2(hv[a]);
+          acc[0] = fma(bb.x, hh.x, fma(bb.y, hh.y, acc[0]));
+          acc[1] = fma(bb.x, hh.y, fma(-bb.y, hh.x, acc[1]));
+        }
+      }
+    }
+    base = ((base | ~ntm) + inc) & ntm;
+    __syncthreads();  // every read of this tile is done before the next one is stored
+  }
+  if (ACC) grid_reduce<2, kPTThreads>(acc, s, res);
+}
+
+// res[0..1] += the sums of the later passes, res[2p..2p+1] for p = 1..npass-1.
+__global__ void k_add_passes(double* res, int npass) {
+  if (threadIdx.x < 2)
+    for (int p = 1; p < npass; ++p) res[threadIdx.x] += res[2 * p + threadIdx.x];
+}
+
 // Window tables of a prepared operator (terms grouped by flip mask; the
 // expectation's coefficients c).  Returns false when the tables would not fit
 // the kernel's shared memory (the quad kernel runs instead).
@@ -574,6 +859,327 @@ int axpy_device(vqc_state h, void* y, const void* x) {
   return VQC_OK;
 }
 
+// Tile passes of a prepared operator (see k_pauli_tile): the groups are
+// reordered by pass; pass p runs groups [gbeg[p], gbeg[p+1]).
+constexpr int kMaxPTPasses = 3;
+constexpr int kPTMinQubits = 18;
+constexpr int kPTNearBits = 5;  // flip masks below bit M + 5 find their partners in L2 in pass 0
+struct PTPlan {
+  std::vector<DevPTPass> passes;
+  std::vector<int> gbeg;
+  std::vector<int> xt;           // per (reordered) group: tile-space flip mask, or -1: partner from global memory
+  std::vector<int64_t> hioff;    // per pass: global offset of each tile high-bit pattern (2^kPTHiBits entries)
+};
+static void plan_pauli_tiles(int nq, int M, int clow, bool write, std::vector<DevGroupW>& groups, PTPlan& pt) {
+  const uint64_t all = nq >= 64 ? ~0ull : ((1ull << nq) - 1), lowm = (1ull << clow) - 1;
+  const int nh = M - clow;
+  std::vector<uint64_t> tmask{((1ull << M) - 1) & all};
+  std::vector<int> pass_of(groups.size(), -1);
+  for (size_t i = 0; i < groups.size(); ++i)
+    if (!(groups[i].x & ~tmask[0])) pass_of[i] = 0;
+  // a further pass covers the high qubits the remaining far flip masks use;
+  // it streams the state once more, so it must take several groups
+  const int min_local = write ? 3 : 2;
+  while ((int)tmask.size() < kMaxPTPasses) {
+    uint64_t U = 0;
+    int nfar = 0;
+    for (size_t i = 0; i < groups.size(); ++i)
+      if (pass_of[i] < 0 && 63 - __builtin_clzll(groups[i].x) >= M + kPTNearBits) {
+        U |= groups[i].x & ~lowm;
+        ++nfar;
+      }
+    if (!nfar) break;
+    uint64_t H = 0;
+    if (__builtin_popcountll(U) <= nh) {
+      H = U;
+      for (int q = nq - 1; q >= clow && __builtin_popcountll(H) < nh; --q) H |= 1ull << q;
+    } else {
+      for (int q = 63; q >= clow && __builtin_popcountll(H) < nh; --q)
+        if (U >> q & 1) H |= 1ull << q;
+    }
+    const uint64_t tm = lowm | H;
+    int nloc = 0;
+    for (size_t i = 0; i < groups.size(); ++i)
+      if (pass_of[i] < 0 && !(groups[i].x & ~tm)) ++nloc;
+    if (nloc < min_local) break;
+    for (size_t i = 0; i < groups.size(); ++i)
+      if (pass_of[i] < 0 && !(groups[i].x & ~tm)) pass_of[i] = (int)tmask.size();
+    tmask.push_back(tm);
+  }
+  for (int& p : pass_of)
+    if (p < 0) p = 0;  // partners from global memory in the first pass
+  std::vector<DevGroupW> reordered;
+  pt.gbeg.assign(1, 0);
+  for (size_t p = 0; p < tmask.size(); ++p) {
+    // tile bit b -> global qubit
+    int tq[64];
+    int nb = 0;
+    for (int q = 0; q < 64; ++q)
+      if (tmask[p] >> q & 1) tq[nb++] = q;
+    for (size_t i = 0; i < groups.size(); ++i) {
+      if (pass_of[i] != (int)p) continue;
+      const uint64_t x = groups[i].x;
+      int xt = -1;
+      if (!(x & ~tmask[p])) {
+        xt = 0;
+        for (int b = 0; b < nb; ++b)
+          if (x >> tq[b] & 1) xt |= 1 << b;
+      }
+      reordered.push_back(groups[i]);
+      pt.xt.push_back(xt);
+    }
+    pt.gbeg.push_back((int)reordered.size());
+    for (int h = 0; h < (1 << kPTHiBits); ++h) {
+      int64_t off = 0;
+      for (int i = 0; i < nh; ++i)
+        if (h >> i & 1) off |= int64_t(1) << tq[clow + i];
+      pt.hioff.push_back(off);
+    }
+    DevPTPass dp;
+    dp.nontile_mask = all & ~tmask[p];
+    dp.ntiles = int64_t(1) << (nq - M);
+    pt.passes.push_back(dp);
+  }
+  groups.swap(reordered);
+}
+
+template <class R, bool WRITE, bool ACC, bool ADD, bool REAL>
+static int pt_launch1(vqc_state h, const void* bra, const void* ket, void* out, const DevPTPass& pass,
+                      const DevGroupW* g, const int* xt, int ng, const int64_t* hioff, const int* shifts,
+                      const void* tables, int nw, const DevTerm* terms, int nt, double dfac, double* res) {
+  auto k = k_pauli_tile<R, WRITE, ACC, ADD, REAL>;
+  const size_t smem = PTLayout<R>(nw, nt, ng).total;
+  VQC_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = (int)std::min<int64_t>(pass.ntiles, (int64_t)device_info(h->device).sms * 2);
+  k<<<grid, kPTThreads, smem, h->stream>>>((const cplx<R>*)bra, (const cplx<R>*)ket, (cplx<R>*)out, h->size(), pass,
+                                           g, xt, ng, hioff, shifts, (const cplx<R>*)tables, nw, terms, nt, dfac,
+                                           h->scr, res);
+  VQC_CK(cudaGetLastError());
+  return VQC_OK;
+}
+template <class R, bool REAL>
+static int pt_launch(vqc_state h, bool write, bool acc, bool add, const void* bra, const void* ket, void* out,
+                     const DevPTPass& pass, const DevGroupW* g, const int* xt, int ng, const int64_t* hioff,
+                     const int* shifts, const void* tables, int nw, const DevTerm* terms, int nt, double dfac,
+                     double* res) {
+#define VQC_PT(W, A, D) \
+  pt_launch1<R, W, A, D, REAL>(h, bra, ket, out, pass, g, xt, ng, hioff, shifts, tables, nw, terms, nt, dfac, res)
+  if (!write) return VQC_PT(false, true, false);
+  if (acc) return add ? VQC_PT(true, true, true) : VQC_PT(true, true, false);
+  return add ? VQC_PT(true, false, true) : VQC_PT(true, false, false);
+#undef VQC_PT
+}
+
+// ----------------------------------------------------------------------------- compiled tile passes
+// k_pauli_tile decodes every group at run time (descriptor and term loads, a
+// loop per group, a switch on the partner permutation).  On states of
+// 2^kPTJitMinQubits amplitudes and more each pass is compiled once per
+// operator structure (NVRTC, cached by source): the groups unrolled, flip
+// masks, Z masks, tile offsets and table shifts as constants, the coefficients
+// of the terms outside the window tables a kernel parameter (new coefficient
+// values reuse the kernel); the window tables stay in shared memory.
+constexpr int kPTJitMinQubits = 20;
+constexpr size_t kPTJitMaxCoefBytes = 30000;  // kernel-parameter space
+
+static int parity64(uint64_t m) { return __builtin_popcountll(m) & 1; }
+
+// Source of one compiled pass; coef receives the parameter values in the
+// order the source reads them.
+static std::string pt_jit_source(bool f32, bool write, bool acc, bool add, bool real, int nw,
+                                 const DevGroupW* groups, const int* xts, int ng, const PauliWin& pw,
+                                 std::vector<double>& coef) {
+  const int M = f32 ? PTCfg<float>::M : PTCfg<double>::M, CLOW = f32 ? PTCfg<float>::CLOW : PTCfg<double>::CLOW;
+  const char* R = f32 ? "float" : "double";
+  std::ostringstream os;
+  coef.clear();
+  std::ostringstream body;
+  for (int gi = 0; gi < ng; ++gi) {
+    const DevGroupW& g = groups[gi];
+    const uint64_t XQ = g.x & ~3ull;
+    const int AX = (int)(g.x & 3);
+    const bool four = g.low0 || g.rlow;
+    body << "      {  // flip mask 0x" << std::hex << g.x << std::dec << "\n";
+    if (xts[gi] >= 0)
+      body << "        const V* p = tile + ((u ^ " << xts[gi] << ") & ~3);\n";
+    else
+      body << "        const V* p = ket + (g ^ " << (long long)XQ << "ll);\n";
+    body << "        V k[4];\n        ld4(p, k);\n";
+    body << "        R fx = 0" << (real ? "" : ", fy = 0") << ";\n";
+    if (four) body << "        R Wx[4] = {0, 0, 0, 0}" << (real ? "" : ", Wy[4] = {0, 0, 0, 0}") << ";\n";
+    int w = g.wbeg;
+    if (g.low0) {
+      body << "        { const V* t = stab + " << w * kWinSize << " + (((unsigned long long)g ^ " << XQ
+           << "ull) & 63);\n          for (int b = 0; b < 4; ++b) { Wx[b] += t[b].x;" << (real ? "" : " Wy[b] += t[b].y;")
+           << " } }\n";
+      ++w;
+    }
+    for (; w < g.wend; ++w)
+      body << "        { const V t = stab[" << w * kWinSize << " + ((((unsigned long long)g ^ " << XQ << "ull) >> "
+           << pw.shifts[w] << ") & 63)]; fx += t.x;" << (real ? "" : " fy += t.y;") << " }\n";
+    for (int q = g.tbeg; q < g.tend; ++q) {
+      const DevTerm& t = pw.rest[q];
+      const uint64_t zh = t.z & ~3ull, zl = t.z & 3;
+      const int cs = parity64(XQ & zh);
+      const int ci = (int)coef.size();
+      coef.push_back(t.c.x);
+      if (!real) coef.push_back(t.c.y);
+      std::string o;
+      if (zh == 0)
+        o = cs ? "true" : "false";
+      else
+        o = std::string("(par((unsigned long long)g & ") + std::to_string((unsigned long long)zh) + "ull)" +
+            (cs ? " ^ 1)" : ")") + " != 0";
+      body << "        { const bool o = " << o << ";\n";
+      body << "          const R ex = o ? -coef.c[" << ci << "] : coef.c[" << ci << "];\n";
+      if (!real) body << "          const R ey = o ? -coef.c[" << ci + 1 << "] : coef.c[" << ci + 1 << "];\n";
+      if (zl == 0) {
+        body << "          fx += ex;" << (real ? "" : " fy += ey;") << " }\n";
+      } else {
+        body << "         ";
+        for (int b = 0; b < 4; ++b) {
+          const bool sb = parity64((uint64_t)b & zl);
+          body << " Wx[" << b << "] " << (sb ? "-=" : "+=") << " ex;";
+          if (!real) body << " Wy[" << b << "] " << (sb ? "-=" : "+=") << " ey;";
+        }
+        body << " }\n";
+      }
+    }
+    // output a takes the partner b = a ^ AX with the phase at b
+    for (int a = 0; a < 4; ++a) {
+      const int b = a ^ AX;
+      const std::string cx = four ? "(Wx[" + std::to_string(b) + "] + fx)" : "fx";
+      const std::string cy = four ? "(Wy[" + std::to_string(b) + "] + fy)" : "fy";
+      if (real) {
+        body << "        h[" << a << "].x = FMA(" << cx << ", k[" << b << "].x, h[" << a << "].x);"
+             << " h[" << a << "].y = FMA(" << cx << ", k[" << b << "].y, h[" << a << "].y);\n";
+      } else {
+        body << "        { const R cx = " << cx << ", cy = " << cy << ";\n"
+             << "          h[" << a << "].x = FMA(cx, k[" << b << "].x, FMA(-cy, k[" << b << "].y, h[" << a << "].x));\n"
+             << "          h[" << a << "].y = FMA(cx, k[" << b << "].y, FMA(cy, k[" << b << "].x, h[" << a << "].y)); }\n";
+      }
+    }
+    body << "      }\n";
+  }
+  const int nc = std::max<int>(1, (int)coef.size());
+  os << "typedef " << R << " R;\ntypedef " << (f32 ? "float2" : "double2") << " V;\n"
+     << "struct Scratch { double* partials; unsigned* counter; double* result; int max_blocks; };\n"
+     << "struct PassT { unsigned long long nontile_mask; long long ntiles; };\n"
+     << "struct Coef { R c[" << nc << "]; };\n"
+     << "#define FMA " << (f32 ? "__fmaf_rn" : "__fma_rn") << "\n"
+     << "__device__ __forceinline__ int par(unsigned long long m) {\n"
+     << "  return (__popc((unsigned)m) ^ __popc((unsigned)(m >> 32))) & 1;\n}\n";
+  if (f32)
+    os << "__device__ __forceinline__ void ld4(const V* p, V (&k)[4]) {\n"
+       << "  const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 2);\n"
+       << "  k[0] = make_float2(a.x, a.y); k[1] = make_float2(a.z, a.w); k[2] = make_float2(b.x, b.y); "
+          "k[3] = make_float2(b.z, b.w);\n}\n"
+       << "__device__ __forceinline__ void st4(V* p, const V (&k)[4]) {\n"
+       << "  *reinterpret_cast<float4*>(p) = make_float4(k[0].x, k[0].y, k[1].x, k[1].y);\n"
+       << "  *reinterpret_cast<float4*>(p + 2) = make_float4(k[2].x, k[2].y, k[3].x, k[3].y);\n}\n";
+  else
+    os << "__device__ __forceinline__ void ld4(const V* p, V (&k)[4]) { for (int a = 0; a < 4; ++a) k[a] = p[a]; }\n"
+       << "__device__ __forceinline__ void st4(V* p, const V (&k)[4]) { for (int a = 0; a < 4; ++a) p[a] = k[a]; }\n";
+  os << "extern \"C\" __global__ void __launch_bounds__(" << kPTThreads << ", 2)\n"
+     << "vqc_pauli(const V* __restrict__ bra, const V* __restrict__ ket, V* __restrict__ out, const PassT pass,\n"
+     << "          const long long* __restrict__ hioff, const V* __restrict__ tables, double dfac, Scratch s,\n"
+     << "          double* res, const __grid_constant__ Coef coef) {\n"
+     << "  constexpr int M = " << M << ", CLOW = " << CLOW << ", T = 1 << M, NT = " << kPTThreads
+     << ", QPT = (T >> 2) / NT, NW = " << nw << ";\n"
+     << "  extern __shared__ __align__(16) unsigned char smem[];\n"
+     << "  V* tile = reinterpret_cast<V*>(smem);\n  V* stab = tile + T;\n"
+     << "  long long* shi = reinterpret_cast<long long*>(stab + NW * 64);\n"
+     << "  __shared__ unsigned long long s_base, s_inc;\n"
+     << "  __shared__ double sred[NT / 32][2];\n  __shared__ bool s_last;\n"
+     << "  for (int i = threadIdx.x; i < NW * 64; i += NT) stab[i] = tables[i];\n"
+     << "  for (int i = threadIdx.x; i < " << (1 << kPTHiBits) << "; i += NT) shi[i] = hioff[i];\n"
+     << "  if (threadIdx.x == 0) {\n"
+     << "    unsigned long long mm = pass.nontile_mask, b0 = 0, inc = 0, t = blockIdx.x, gd = gridDim.x;\n"
+     << "    while (mm) {\n      const unsigned long long low = mm & (~mm + 1);\n"
+     << "      if (t & 1) b0 |= low;\n      if (gd & 1) inc |= low;\n"
+     << "      t >>= 1; gd >>= 1; mm ^= low;\n    }\n    s_base = b0; s_inc = inc;\n  }\n"
+     << "  __syncthreads();\n"
+     << "  const unsigned long long ntm = pass.nontile_mask, inc = s_inc;\n"
+     << "  unsigned long long base = s_base;\n"
+     << "  double acc0 = 0, acc1 = 0;\n"
+     << "  for (long long tl = blockIdx.x; tl < pass.ntiles; tl += gridDim.x) {\n"
+     << "#pragma unroll\n    for (int kq = 0; kq < QPT; ++kq) {\n"
+     << "      const int u = (threadIdx.x + kq * NT) << 2;\n"
+     << "      const long long g = (long long)base + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));\n"
+     << "      V k[4];\n      ld4(ket + g, k);\n      st4(tile + u, k);\n    }\n"
+     << "    __syncthreads();\n"
+     << "#pragma unroll 1\n    for (int kq = 0; kq < QPT; ++kq) {\n"
+     << "      const int u = (threadIdx.x + kq * NT) << 2;\n"
+     << "      const long long g = (long long)base + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));\n"
+     << "      V h[4];\n      for (int a = 0; a < 4; ++a) h[a].x = h[a].y = 0;\n"
+     << body.str();
+  if (write) {
+    os << "      {\n        const R df = (R)dfac;\n        V o[4];\n"
+       << "        for (int a = 0; a < 4; ++a) { o[a].x = df * h[a].x; o[a].y = df * h[a].y; }\n";
+    if (add)
+      os << "        V pv[4];\n        ld4(out + g, pv);\n"
+         << "        for (int a = 0; a < 4; ++a) { o[a].x += pv[a].x; o[a].y += pv[a].y; }\n";
+    os << "        st4(out + g, o);\n      }\n";
+  }
+  if (acc)
+    os << "      {\n        V bv[4];\n        if (bra == ket) ld4(tile + u, bv); else ld4(bra + g, bv);\n"
+       << "        for (int a = 0; a < 4; ++a) {\n"
+       << "          const double bx = bv[a].x, by = bv[a].y, hx = h[a].x, hy = h[a].y;\n"
+       << "          acc0 = __fma_rn(bx, hx, __fma_rn(by, hy, acc0));\n"
+       << "          acc1 = __fma_rn(bx, hy, __fma_rn(-by, hx, acc1));\n"
+       << "        }\n      }\n";
+  os << "    }\n    base = ((base | ~ntm) + inc) & ntm;\n    __syncthreads();\n  }\n";
+  if (acc) {
+    // the deterministic grid reduction: block sums in warp order, then the
+    // last block adds the block partials in block order
+    os << "  {\n    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n"
+       << "    double v0 = acc0, v1 = acc1;\n"
+       << "    for (int o = 16; o > 0; o >>= 1) { v0 += __shfl_xor_sync(0xffffffffu, v0, o);"
+          " v1 += __shfl_xor_sync(0xffffffffu, v1, o); }\n"
+       << "    if (lane == 0) { sred[warp][0] = v0; sred[warp][1] = v1; }\n    __syncthreads();\n"
+       << "    if (threadIdx.x < 2) {\n      double v = 0;\n"
+       << "      for (int w = 0; w < NT / 32; ++w) v += sred[w][threadIdx.x];\n"
+       << "      s.partials[(unsigned long long)blockIdx.x * " << kMaxAcc << " + threadIdx.x] = v;\n    }\n"
+       << "    __threadfence();\n    __syncthreads();\n"
+       << "    if (threadIdx.x == 0) s_last = (atomicAdd(s.counter, 1u) == gridDim.x - 1);\n"
+       << "    __syncthreads();\n    if (!s_last) return;\n    __threadfence();\n"
+       << "    for (int i = 0; i < 2; ++i) {\n      double v = 0;\n"
+       << "      for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) v += __ldcg(&s.partials[(unsigned long long)b * "
+       << kMaxAcc << " + i]);\n"
+       << "      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);\n"
+       << "      __syncthreads();\n      if (lane == 0) sred[warp][0] = v;\n      __syncthreads();\n"
+       << "      if (threadIdx.x == 0) {\n        double t = 0;\n"
+       << "        for (int w = 0; w < NT / 32; ++w) t += sred[w][0];\n        res[i] = t;\n      }\n    }\n"
+       << "    if (threadIdx.x == 0) *s.counter = 0;\n  }\n";
+  }
+  os << "}\n";
+  return os.str();
+}
+
+// Launches a compiled pass (kernel from jit_kernels, name vqc_pauli).
+static int pt_jit_launch(vqc_state h, const void* kernel, bool f32, const void* bra, const void* ket, void* out,
+                         const DevPTPass& pass, const int64_t* hioff, const void* tables, int nw, double dfac,
+                         double* res, const std::vector<double>& coef) {
+  const size_t amp = f32 ? 8 : 16;
+  const size_t smem = (amp << (f32 ? PTCfg<float>::M : PTCfg<double>::M)) + (size_t)nw * kWinSize * amp +
+                      sizeof(int64_t) * (size_t(1) << kPTHiBits);
+  VQC_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = (int)std::min<int64_t>(pass.ntiles, (int64_t)device_info(h->device).sms * 2);
+  std::vector<unsigned char> cb(std::max<size_t>(1, coef.size()) * (f32 ? 4 : 8), 0);
+  for (size_t i = 0; i < coef.size(); ++i) {
+    if (f32) {
+      const float v = (float)coef[i];
+      std::memcpy(cb.data() + 4 * i, &v, 4);
+    } else {
+      std::memcpy(cb.data() + 8 * i, &coef[i], 8);
+    }
+  }
+  Scratch s = h->scr;
+  void* args[] = {(void*)&bra, (void*)&ket, (void*)&out, (void*)&pass, (void*)&hioff, (void*)&tables,
+                  (void*)&dfac, (void*)&s, (void*)&res, (void*)cb.data()};
+  VQC_CK(cudaLaunchKernel(kernel, dim3(grid), dim3(kPTThreads), args, smem, h->stream));
+  return VQC_OK;
+}
+
 // Runs the Pauli kernel in chunks of at most kMaxTermsPerLaunch terms; the
 // expectation (if any) is summed on the host in FP64 over chunks.
 int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vqc_pauli* terms, int nterms,
@@ -604,6 +1210,26 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
     }
     PauliWin pw;
     const bool win = quad && !sep && build_windows(p.groups, p.terms, h->amp_bytes(), pw);
+    // tile passes (k_pauli_tile) for states of 2^kPTMinQubits amplitudes and
+    // more whose operator has window tables (VQC_PAULI_TILE=0: one pass with
+    // every partner read from global memory)
+    PTPlan pt;
+    bool tiled = false, real = false;
+    if (win && h->nq >= kPTMinQubits && env_on("VQC_PAULI_TILE", true)) {
+      const bool f32 = h->amp_bytes() == 8;
+      const size_t need = f32 ? PTLayout<float>((int)pw.shifts.size(), (int)pw.rest.size(), (int)pw.groups.size()).total
+                              : PTLayout<double>((int)pw.shifts.size(), (int)pw.rest.size(), (int)pw.groups.size()).total;
+      if (need <= (size_t)device_info(h->device).max_smem_optin) {
+        tiled = true;
+        plan_pauli_tiles(h->nq, f32 ? PTCfg<float>::M : PTCfg<double>::M, f32 ? PTCfg<float>::CLOW : PTCfg<double>::CLOW,
+                         write, pw.groups, pt);
+        real = true;
+        for (const cd& v : pw.tables)
+          if (v.imag() != 0) real = false;
+        for (const DevTerm& t : pw.rest)
+          if (t.c.y != 0) real = false;
+      }
+    }
     // VQC_PAULI_SPLIT=1: groups whose flip masks reach beyond the amplitudes one
     // wave of the grid covers (the XXZ chain's top pairs on a state larger than
     // L2) run in a second launch whose traversal puts the top bits in the fast
@@ -613,7 +1239,7 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
     // so one launch is the default.
     const int grid = reduction_grid(h->device, h->size());
     int nlow = (int)pw.groups.size(), tlo = 0, ths = 0, thl = 0;
-    if (win && h->nq >= 20 && env_on("VQC_PAULI_SPLIT", false)) {
+    if (win && !tiled && h->nq >= 20 && env_on("VQC_PAULI_SPLIT", false)) {
       const int nq4 = h->nq - 2, tlo_ = 5;
       int wave = 0;
       while ((int64_t(2) << wave) <= (int64_t)grid * kRedThreads) ++wave;  // quad bits one wave covers
@@ -663,7 +1289,14 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
                           : (quad ? sizeof(DevGroup4) * g4.size() : sizeof(DevGroup) * p.groups.size()),
                  shb = win ? sizeof(int) * ((pw.shifts.size() + 3) & ~size_t(3)) : 0,
                  tb = sizeof(DevTerm) * (win ? pw.rest.size() : p.terms.size());
-    std::vector<unsigned char> buf(wtb + gb + shb + tb, 0);
+    // tile passes: [flip masks in tile space][high-bit offset tables] after the rest
+    const size_t xtb = tiled ? ((sizeof(int) * pt.xt.size() + 15) & ~size_t(15)) : 0,
+                 hob = tiled ? sizeof(int64_t) * pt.hioff.size() : 0;
+    std::vector<unsigned char> buf(wtb + gb + shb + tb + xtb + hob, 0);
+    if (tiled) {
+      std::memcpy(buf.data() + wtb + gb + shb + tb, pt.xt.data(), sizeof(int) * pt.xt.size());
+      std::memcpy(buf.data() + wtb + gb + shb + tb + xtb, pt.hioff.data(), hob);
+    }
     if (win) {
       for (size_t i = 0; i < pw.tables.size(); ++i) {
         if (amp == 8) {
@@ -696,11 +1329,46 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
       if ((rc = workspace(h, 3, w3))) return rc;
       target = w3[2];
     }
+    // compiled tile passes (nullptr: the generic tile kernel runs that pass)
+    std::vector<const void*> ptk;
+    std::vector<std::vector<double>> ptc;
+    if (tiled && h->nq >= kPTJitMinQubits && jit_mode() != 0 && jit_available()) {
+      const bool f32 = amp == 8;
+      std::vector<std::string> srcs;
+      for (size_t pp = 0; pp < pt.passes.size(); ++pp) {
+        const int g0 = pt.gbeg[pp], ngp = pt.gbeg[pp + 1] - g0;
+        std::vector<double> c;
+        srcs.push_back(pt_jit_source(f32, write, acc, pp > 0, real, nw, pw.groups.data() + g0, pt.xt.data() + g0, ngp,
+                                     pw, c));
+        if (c.size() * (f32 ? 4 : 8) > kPTJitMaxCoefBytes) srcs.back().clear();
+        ptc.push_back(std::move(c));
+      }
+      if ((rc = jit_kernels(srcs, ptk, "vqc_pauli"))) return rc;
+    }
     ProfScope prof(h->stream, write ? "pauli_apply" : "pauli_expect",
                    (double)h->size() * h->amp_bytes() * (1 + (write ? 1 : 0) + (acc && bra != ket ? 1 : 0)));
 #define VQC_PAULI_LAUNCH(R)                                                                                      \
   do {                                                                                                           \
-    if (win) {                                                                                                   \
+    if (tiled) {                                                                                                 \
+      const DevGroupW* gw = (const DevGroupW*)(ob + wtb);                                                        \
+      const int* xts = (const int*)(ob + wtb + gb + shb + tb);                                                   \
+      const int64_t* hio = (const int64_t*)(ob + wtb + gb + shb + tb + xtb);                                     \
+      const int np = (int)pt.passes.size();                                                                      \
+      for (int pp = 0; pp < np; ++pp) {                                                                          \
+        const int g0 = pt.gbeg[pp], ngp = pt.gbeg[pp + 1] - g0;                                                  \
+        if (pp < (int)ptk.size() && ptk[pp])                                                                     \
+          rc = pt_jit_launch(h, ptk[pp], sizeof(R) == 4, bra, ket, target, pt.passes[pp],                        \
+                             hio + ((size_t)pp << kPTHiBits), ob, nw, hermitian_part ? 2.0 : 1.0,                \
+                             h->scr.result + 2 * pp, ptc[pp]);                                                   \
+        else                                                                                                     \
+          rc = (real ? pt_launch<R, true> : pt_launch<R, false>)(                                                \
+              h, write, acc, pp > 0, bra, ket, target, pt.passes[pp], gw + g0, xts + g0, ngp,                    \
+              hio + ((size_t)pp << kPTHiBits), (const int*)(ob + wtb + gb), ob, nw, dt, nt,                      \
+              hermitian_part ? 2.0 : 1.0, h->scr.result + 2 * pp);                                               \
+        if (rc) return rc;                                                                                       \
+      }                                                                                                          \
+      if (acc && np > 1) k_add_passes<<<1, 32, 0, h->stream>>>(h->scr.result, np);                              \
+    } else if (win) {                                                                                            \
       const DevGroupW* gw = (const DevGroupW*)(ob + wtb);                                                        \
       const int nhigh = (int)pw.groups.size() - nlow;                                                            \
       auto k1 = write ? (acc ? k_pauli_win<R, true, true, false> : k_pauli_win<R, true, false, false>)           \
