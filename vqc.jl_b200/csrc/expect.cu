@@ -464,26 +464,31 @@ struct PTLayout {
   }
 };
 
-// Four amplitudes of a tile quad (16-byte aligned) from / to shared memory.
-template <class V>
-__device__ __forceinline__ void tile_ld4(const V* t, V (&kv)[4]) {
+// The tile in shared memory as 16-byte planes: a quad's four amplitudes are
+// one 16-byte element in each of 2 (FP32) or 4 (FP64) planes of NQ elements,
+// so the lanes of a warp reading consecutive quads (or a permutation of them)
+// touch consecutive 16-byte words: no bank conflicts.
+template <class V, int NQ>
+__device__ __forceinline__ void tile_ld4(const V* t, int q, V (&kv)[4]) {
+  const float4* f = reinterpret_cast<const float4*>(t);
   if constexpr (sizeof(V) == 8) {
-    const float4 a = *reinterpret_cast<const float4*>(t), b = *reinterpret_cast<const float4*>(t + 2);
+    const float4 a = f[q], b = f[NQ + q];
     kv[0] = make_float2(a.x, a.y), kv[1] = make_float2(a.z, a.w);
     kv[2] = make_float2(b.x, b.y), kv[3] = make_float2(b.z, b.w);
   } else {
 #pragma unroll
-    for (int a = 0; a < 4; ++a) kv[a] = t[a];
+    for (int a = 0; a < 4; ++a) kv[a] = t[a * NQ + q];
   }
 }
-template <class V>
-__device__ __forceinline__ void tile_st4(V* t, const V (&kv)[4]) {
+template <class V, int NQ>
+__device__ __forceinline__ void tile_st4(V* t, int q, const V (&kv)[4]) {
+  float4* f = reinterpret_cast<float4*>(t);
   if constexpr (sizeof(V) == 8) {
-    *reinterpret_cast<float4*>(t) = make_float4(kv[0].x, kv[0].y, kv[1].x, kv[1].y);
-    *reinterpret_cast<float4*>(t + 2) = make_float4(kv[2].x, kv[2].y, kv[3].x, kv[3].y);
+    f[q] = make_float4(kv[0].x, kv[0].y, kv[1].x, kv[1].y);
+    f[NQ + q] = make_float4(kv[2].x, kv[2].y, kv[3].x, kv[3].y);
   } else {
 #pragma unroll
-    for (int a = 0; a < 4; ++a) t[a] = kv[a];
+    for (int a = 0; a < 4; ++a) t[a * NQ + q] = kv[a];
   }
 }
 
@@ -563,9 +568,20 @@ __global__ void __launch_bounds__(kPTThreads, 2)
       V kv[4];
       if (!VQC_DCHECK(gqk + 3, N)) continue;
       load4<R>(ket + gqk, kv);
-      tile_st4(tile + u, kv);
+      tile_st4<V, (T >> 2)>(tile, u >> 2, kv);
     }
     __syncthreads();
+    if (tl + gridDim.x < pass.ntiles) {
+      // the next tile's amplitudes (and output words) into L2 while this one is computed
+      const uint64_t nb = ((base | ~ntm) + inc) & ntm;
+#pragma unroll
+      for (int k = 0; k < QPT; ++k) {
+        const int u = (threadIdx.x + k * kPTThreads) << 2;
+        const int64_t g = (int64_t)nb + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(ket + g));
+        if (ADD) asm volatile("prefetch.global.L2 [%0];" ::"l"(out + g));
+      }
+    }
     // one quad at a time (four accumulators: the group loop's registers stay few)
 #pragma unroll 1
     for (int k = 0; k < QPT; ++k) {
@@ -583,7 +599,7 @@ __global__ void __launch_bounds__(kPTThreads, 2)
         if (xt >= 0) {
           const int ub = (u ^ xt) & ~3;
           if (!VQC_DCHECK(ub + 3, T)) continue;
-          tile_ld4(tile + ub, kv);
+          tile_ld4<V, (T >> 2)>(tile, ub >> 2, kv);
         } else {
           if (!VQC_DCHECK(jb + 3, N)) continue;
           load4<R>(ket + jb, kv);
@@ -680,7 +696,7 @@ __global__ void __launch_bounds__(kPTThreads, 2)
       if (ACC) {
         V b[4];
         if (bra == ket) {
-          tile_ld4(tile + u, b);
+          tile_ld4<V, (T >> 2)>(tile, u >> 2, b);
         } else {
           load4<R>(bra + gqk, b);
         }
@@ -983,11 +999,23 @@ constexpr size_t kPTJitMaxCoefBytes = 30000;  // kernel-parameter space
 
 static int parity64(uint64_t m) { return __builtin_popcountll(m) & 1; }
 
+// Block shape of the compiled passes: 256 threads, three CTAs per SM (a CTA
+// loading its tile overlaps the others' compute), or 512 threads, two CTAs
+// (VQC_PAULI_NT=512).
+struct PTJitShape {
+  int threads, per_sm;
+};
+static PTJitShape pt_jit_shape() {
+  const char* v = std::getenv("VQC_PAULI_NT");
+  if (v && *v && std::atoi(v) == 512) return {512, 2};
+  return {256, 3};
+}
+
 // Source of one compiled pass; coef receives the parameter values in the
 // order the source reads them.
 static std::string pt_jit_source(bool f32, bool write, bool acc, bool add, bool real, int nw,
                                  const DevGroupW* groups, const int* xts, int ng, const PauliWin& pw,
-                                 std::vector<double>& coef) {
+                                 std::vector<double>& coef, const PTJitShape& shape) {
   const int M = f32 ? PTCfg<float>::M : PTCfg<double>::M, CLOW = f32 ? PTCfg<float>::CLOW : PTCfg<double>::CLOW;
   const char* R = f32 ? "float" : "double";
   std::ostringstream os;
@@ -1000,10 +1028,9 @@ static std::string pt_jit_source(bool f32, bool write, bool acc, bool add, bool 
     const bool four = g.low0 || g.rlow;
     body << "      {  // flip mask 0x" << std::hex << g.x << std::dec << "\n";
     if (xts[gi] >= 0)
-      body << "        const V* p = tile + ((u ^ " << xts[gi] << ") & ~3);\n";
+      body << "        V k[4];\n        tld4(tile, (u ^ " << xts[gi] << ") >> 2, k);\n";
     else
-      body << "        const V* p = ket + (g ^ " << (long long)XQ << "ll);\n";
-    body << "        V k[4];\n        ld4(p, k);\n";
+      body << "        V k[4];\n        ld4(ket + (g ^ " << (long long)XQ << "ll), k);\n";
     body << "        R fx = 0" << (real ? "" : ", fy = 0") << ";\n";
     if (four) body << "        R Wx[4] = {0, 0, 0, 0}" << (real ? "" : ", Wy[4] = {0, 0, 0, 0}") << ";\n";
     int w = g.wbeg;
@@ -1079,11 +1106,27 @@ static std::string pt_jit_source(bool f32, bool write, bool acc, bool add, bool 
   else
     os << "__device__ __forceinline__ void ld4(const V* p, V (&k)[4]) { for (int a = 0; a < 4; ++a) k[a] = p[a]; }\n"
        << "__device__ __forceinline__ void st4(V* p, const V (&k)[4]) { for (int a = 0; a < 4; ++a) p[a] = k[a]; }\n";
-  os << "extern \"C\" __global__ void __launch_bounds__(" << kPTThreads << ", 2)\n"
+  // the tile as 16-byte planes (quad q: one element per plane), bank-conflict free
+  const int nq4 = 1 << (M - 2);
+  if (f32)
+    os << "__device__ __forceinline__ void tld4(const V* t, int q, V (&k)[4]) {\n"
+       << "  const float4 a = reinterpret_cast<const float4*>(t)[q], b = reinterpret_cast<const float4*>(t)[" << nq4
+       << " + q];\n"
+       << "  k[0] = make_float2(a.x, a.y); k[1] = make_float2(a.z, a.w); k[2] = make_float2(b.x, b.y); "
+          "k[3] = make_float2(b.z, b.w);\n}\n"
+       << "__device__ __forceinline__ void tst4(V* t, int q, const V (&k)[4]) {\n"
+       << "  reinterpret_cast<float4*>(t)[q] = make_float4(k[0].x, k[0].y, k[1].x, k[1].y);\n"
+       << "  reinterpret_cast<float4*>(t)[" << nq4 << " + q] = make_float4(k[2].x, k[2].y, k[3].x, k[3].y);\n}\n";
+  else
+    os << "__device__ __forceinline__ void tld4(const V* t, int q, V (&k)[4]) { for (int a = 0; a < 4; ++a) k[a] = t[a * "
+       << nq4 << " + q]; }\n"
+       << "__device__ __forceinline__ void tst4(V* t, int q, const V (&k)[4]) { for (int a = 0; a < 4; ++a) t[a * " << nq4
+       << " + q] = k[a]; }\n";
+  os << "extern \"C\" __global__ void __launch_bounds__(" << shape.threads << ", " << shape.per_sm << ")\n"
      << "vqc_pauli(const V* __restrict__ bra, const V* __restrict__ ket, V* __restrict__ out, const PassT pass,\n"
      << "          const long long* __restrict__ hioff, const V* __restrict__ tables, double dfac, Scratch s,\n"
      << "          double* res, const __grid_constant__ Coef coef) {\n"
-     << "  constexpr int M = " << M << ", CLOW = " << CLOW << ", T = 1 << M, NT = " << kPTThreads
+     << "  constexpr int M = " << M << ", CLOW = " << CLOW << ", T = 1 << M, NT = " << shape.threads
      << ", QPT = (T >> 2) / NT, NW = " << nw << ";\n"
      << "  extern __shared__ __align__(16) unsigned char smem[];\n"
      << "  V* tile = reinterpret_cast<V*>(smem);\n  V* stab = tile + T;\n"
@@ -1105,8 +1148,16 @@ static std::string pt_jit_source(bool f32, bool write, bool acc, bool add, bool 
      << "#pragma unroll\n    for (int kq = 0; kq < QPT; ++kq) {\n"
      << "      const int u = (threadIdx.x + kq * NT) << 2;\n"
      << "      const long long g = (long long)base + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));\n"
-     << "      V k[4];\n      ld4(ket + g, k);\n      st4(tile + u, k);\n    }\n"
+     << "      V k[4];\n      ld4(ket + g, k);\n      tst4(tile, u >> 2, k);\n    }\n"
      << "    __syncthreads();\n"
+     << "    if (tl + gridDim.x < pass.ntiles) {\n"
+     << "      const unsigned long long nb = ((base | ~ntm) + inc) & ntm;\n"
+     << "#pragma unroll\n      for (int kq = 0; kq < QPT; ++kq) {\n"
+     << "        const int u = (threadIdx.x + kq * NT) << 2;\n"
+     << "        const long long g = (long long)nb + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));\n"
+     << "        asm volatile(\"prefetch.global.L2 [%0];\" ::\"l\"(ket + g));\n"
+     << (add ? "        asm volatile(\"prefetch.global.L2 [%0];\" ::\"l\"(out + g));\n" : "")
+     << "      }\n    }\n"
      << "#pragma unroll 1\n    for (int kq = 0; kq < QPT; ++kq) {\n"
      << "      const int u = (threadIdx.x + kq * NT) << 2;\n"
      << "      const long long g = (long long)base + shi[u >> CLOW] + (u & ((1 << CLOW) - 1));\n"
@@ -1121,7 +1172,7 @@ static std::string pt_jit_source(bool f32, bool write, bool acc, bool add, bool 
     os << "        st4(out + g, o);\n      }\n";
   }
   if (acc)
-    os << "      {\n        V bv[4];\n        if (bra == ket) ld4(tile + u, bv); else ld4(bra + g, bv);\n"
+    os << "      {\n        V bv[4];\n        if (bra == ket) tld4(tile, u >> 2, bv); else ld4(bra + g, bv);\n"
        << "        for (int a = 0; a < 4; ++a) {\n"
        << "          const double bx = bv[a].x, by = bv[a].y, hx = h[a].x, hy = h[a].y;\n"
        << "          acc0 = __fma_rn(bx, hx, __fma_rn(by, hy, acc0));\n"
@@ -1158,12 +1209,12 @@ static std::string pt_jit_source(bool f32, bool write, bool acc, bool add, bool 
 // Launches a compiled pass (kernel from jit_kernels, name vqc_pauli).
 static int pt_jit_launch(vqc_state h, const void* kernel, bool f32, const void* bra, const void* ket, void* out,
                          const DevPTPass& pass, const int64_t* hioff, const void* tables, int nw, double dfac,
-                         double* res, const std::vector<double>& coef) {
+                         double* res, const std::vector<double>& coef, const PTJitShape& shape) {
   const size_t amp = f32 ? 8 : 16;
   const size_t smem = (amp << (f32 ? PTCfg<float>::M : PTCfg<double>::M)) + (size_t)nw * kWinSize * amp +
                       sizeof(int64_t) * (size_t(1) << kPTHiBits);
   VQC_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = (int)std::min<int64_t>(pass.ntiles, (int64_t)device_info(h->device).sms * 2);
+  const int grid = (int)std::min<int64_t>(pass.ntiles, (int64_t)device_info(h->device).sms * shape.per_sm);
   std::vector<unsigned char> cb(std::max<size_t>(1, coef.size()) * (f32 ? 4 : 8), 0);
   for (size_t i = 0; i < coef.size(); ++i) {
     if (f32) {
@@ -1176,7 +1227,7 @@ static int pt_jit_launch(vqc_state h, const void* kernel, bool f32, const void* 
   Scratch s = h->scr;
   void* args[] = {(void*)&bra, (void*)&ket, (void*)&out, (void*)&pass, (void*)&hioff, (void*)&tables,
                   (void*)&dfac, (void*)&s, (void*)&res, (void*)cb.data()};
-  VQC_CK(cudaLaunchKernel(kernel, dim3(grid), dim3(kPTThreads), args, smem, h->stream));
+  VQC_CK(cudaLaunchKernel(kernel, dim3(grid), dim3(shape.threads), args, smem, h->stream));
   return VQC_OK;
 }
 
@@ -1332,6 +1383,7 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
     // compiled tile passes (nullptr: the generic tile kernel runs that pass)
     std::vector<const void*> ptk;
     std::vector<std::vector<double>> ptc;
+    const PTJitShape pshape = pt_jit_shape();
     if (tiled && h->nq >= kPTJitMinQubits && jit_mode() != 0 && jit_available()) {
       const bool f32 = amp == 8;
       std::vector<std::string> srcs;
@@ -1339,7 +1391,7 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
         const int g0 = pt.gbeg[pp], ngp = pt.gbeg[pp + 1] - g0;
         std::vector<double> c;
         srcs.push_back(pt_jit_source(f32, write, acc, pp > 0, real, nw, pw.groups.data() + g0, pt.xt.data() + g0, ngp,
-                                     pw, c));
+                                     pw, c, pshape));
         if (c.size() * (f32 ? 4 : 8) > kPTJitMaxCoefBytes) srcs.back().clear();
         ptc.push_back(std::move(c));
       }
@@ -1359,7 +1411,7 @@ int pauli_run(vqc_state h, const void* bra, const void* ket, void* out, const vq
         if (pp < (int)ptk.size() && ptk[pp])                                                                     \
           rc = pt_jit_launch(h, ptk[pp], sizeof(R) == 4, bra, ket, target, pt.passes[pp],                        \
                              hio + ((size_t)pp << kPTHiBits), ob, nw, hermitian_part ? 2.0 : 1.0,                \
-                             h->scr.result + 2 * pp, ptc[pp]);                                                   \
+                             h->scr.result + 2 * pp, ptc[pp], pshape);                                           \
         else                                                                                                     \
           rc = (real ? pt_launch<R, true> : pt_launch<R, false>)(                                                \
               h, write, acc, pp > 0, bra, ket, target, pt.passes[pp], gw + g0, xts + g0, ngp,                    \

@@ -329,8 +329,9 @@ static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype, bool 
 // of the packed layout).  The free bits left over are filled preferring the
 // stage's control bits (register controls are compile-time cases in the FP32
 // body), then a bank-conflict-free layout.
-static void plan_stages(PlanPass& p, int M, int dtype, bool packed) {
+static void plan_stages(PlanPass& p, int M, int dtype, bool packed, int rb = kRegBits) {
   const bool lane0 = packed;
+  p.stages.clear();
   std::map<int, int> tbit;  // global qubit -> tile bit
   for (int b = 0; b < (int)p.tile_q.size(); ++b) tbit[p.tile_q[b]] = b;
   std::vector<int> pending(p.ops.size());
@@ -354,7 +355,7 @@ static void plan_stages(PlanPass& p, int M, int dtype, bool packed) {
       std::vector<int> u = rs;
       for (int b : need)
         if (std::find(u.begin(), u.end(), b) == u.end()) u.push_back(b);
-      if ((int)u.size() <= kRegBits) {
+      if ((int)u.size() <= rb) {
         rs = u;
         st.ops.push_back(oi);
       } else {
@@ -376,7 +377,7 @@ static void plan_stages(PlanPass& p, int M, int dtype, bool packed) {
     for (int b = 0; b < M; ++b)
       if (std::find(rs.begin(), rs.end(), b) == rs.end() && std::find(cand.begin(), cand.end(), b) == cand.end())
         cand.push_back(b);
-    const int need_more = kRegBits - (int)rs.size();
+    const int need_more = rb - (int)rs.size();
     std::vector<int> best;
     bool found = false;
     const int nc = std::min((int)cand.size(), 10);
@@ -538,15 +539,16 @@ static double pass_fma_ops(const PlanPass& p, int n, bool adj, bool packed) {
 static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint64_t tile_mask,
                       std::map<int, int>& tbit, bool adj, int& slot, int row, std::vector<DevStageF>& ds,
                       std::vector<DevOp>& dops, std::vector<float2>& pool, size_t pool_begin,
-                      std::vector<AccRef>* accs) {
+                      std::vector<AccRef>* accs, int rb) {
   DevStageF s{};
   const std::vector<int>& rs = st.rs;  // ascending, rs[0] = tile bit 0
+  const int na = 1 << rb, np = na / 2;  // register amplitudes, pairs
   uint32_t rsmask = 0;
   for (int b : rs) rsmask |= 1u << b;
-  uint32_t dep[16];
-  for (int j = 0; j < 16; ++j) {
+  uint32_t dep[32];
+  for (int j = 0; j < na; ++j) {
     uint32_t t = 0;
-    for (int i = 0; i < kRegBits; ++i)
+    for (int i = 0; i < rb; ++i)
       if (j >> i & 1) t |= 1u << rs[i];
     dep[j] = t;
     s.dep[j] = t;
@@ -569,7 +571,7 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
       s.swt[k][nib] = f32t::swz_pair(t >> 1);
       s.gthr[k][nib] = gq(t);
     }
-  for (int m = 0; m < 8; ++m) {
+  for (int m = 0; m < np; ++m) {
     s.swm[m] = f32t::swz_pair(dep[2 * m] >> 1);
     s.gdep[m] = gq(dep[2 * m]);
   }
@@ -600,7 +602,7 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
       }
     }
     uint32_t rmask = 0;
-    for (int j = 0; j < 16; ++j) {
+    for (int j = 0; j < na; ++j) {
       bool ok = true;
       for (auto& c : rc) ok = ok && ((j >> c.first & 1) == c.second);
       if (ok) rmask |= 1u << j;
@@ -614,7 +616,7 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
     o.mat = (int)(pool.size() - pool_begin);
     if (f.kind == kOpU1) {
       const int tb = jbit(tbit[f.tq[0]]), form = u1_form(f.mat);
-      o.code |= (tb << 4) | (form << 11) | (rctl << 16);
+      o.code |= op_r_bits(tb, 0) | (form << 11) | (rctl << 16);
       if (adj && f.acc) o.code |= (acc_kind(f) << 14) | (acc_anti_hermitian(f) ? kCodeAH : 0);
       const cd u00 = f.mat[0], u01 = f.mat[1], u10 = f.mat[2], u11 = f.mat[3];
       if (tb != 0) {
@@ -650,7 +652,7 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
         }
       }
     } else {
-      if (f.kind == kOpU2) o.code |= (jbit(tbit[f.tq[0]]) << 4) | (jbit(tbit[f.tq[1]]) << 6);
+      if (f.kind == kOpU2) o.code |= op_r_bits(jbit(tbit[f.tq[0]]), jbit(tbit[f.tq[1]]));
       for (const cd& c : f.mat) put(c.real(), c.imag());
     }
     o.nd = f.nd;
@@ -686,7 +688,7 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
 
 template <class R, int M, bool ADJ>
 static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, SerialPlan& sp, std::vector<AccRef>* accs,
-                           bool packed = false) {
+                           bool packed = false, int rb = kRegBits) {
   Device d;
   std::vector<cplx<R>> pool;
   std::vector<PassLoc>& locs = sp.locs;
@@ -699,7 +701,7 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
       locs[pi].gate = p.gate;
       continue;
     }
-    plan_stages(p, M, dtype, packed);
+    plan_stages(p, M, dtype, packed, rb);
     std::vector<DevStage> ds;
     std::vector<DevOp> dops;
     std::map<int, int> tbit;
@@ -713,7 +715,7 @@ static void serialize_plan(int n, int dtype, std::vector<PlanPass>& passes, Seri
     for (const PlanStage& st : p.stages) {
       if constexpr (std::is_same<R, float>::value) {
         if (packed) {
-          stage_f32(p, st, M, n, tile_mask, tbit, ADJ, slot, row, dsf, dops, pool, pool_begin, accs);
+          stage_f32(p, st, M, n, tile_mask, tbit, ADJ, slot, row, dsf, dops, pool, pool_begin, accs, rb);
           continue;
         }
       }
@@ -850,9 +852,9 @@ static void note_plan(bool adj, const std::vector<PlanPass>& passes) {
 }
 
 template <int M, bool ADJ>
-static int jit_grid(int device, const void* k, const PassShape& ps) {
-  constexpr int NT = 1 << (M - kRegBits);
-  const size_t smem = pass_smem<float, M, ADJ>(ps) + jit_extra_smem(ADJ, M);
+static int jit_grid(int device, const void* k, const PassShape& ps, int rb = kRegBits) {
+  const int NT = 1 << (M - rb);
+  const size_t smem = pass_smem<float, M, ADJ>(ps) + jit_extra_smem(ADJ, M, rb);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem) != cudaSuccess || per_sm < 1) {
@@ -865,9 +867,9 @@ static int jit_grid(int device, const void* k, const PassShape& ps) {
 template <int M, bool ADJ>
 static int launch_tile_jit(vqc_state h, const void* k, void* psi, void* lam, const DevPass* dp, const void* ds,
                            const DevOp* dops, const void* pool, double* partials, int grid, const PassShape& ps,
-                           const void* host_pool, double flops) {
-  constexpr int NT = 1 << (M - kRegBits);
-  const size_t smem = pass_smem<float, M, ADJ>(ps) + jit_extra_smem(ADJ, M);
+                           const void* host_pool, double flops, int rb = kRegBits) {
+  const int NT = 1 << (M - rb);
+  const size_t smem = pass_smem<float, M, ADJ>(ps) + jit_extra_smem(ADJ, M, rb);
   VQC_CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
   ProfScope prof(h->stream, ADJ ? "tile_adjoint" : "tile_forward", (double)(ADJ ? 4 : 2) * h->size() * sizeof(float2),
                  flops);
@@ -886,6 +888,11 @@ static bool use_jit(const vqc_state h) {
 // The packed FP32 plan layout: for the compiled passes, or forced with
 // VQC_JIT=interp (the packed interpreter, the compiled kernels' fallback).
 static bool use_packed(const vqc_state h) { return h->dtype == VQC_C64 && (use_jit(h) || jit_mode() == 3); }
+// VQC_JIT_WIDE=0: the compiled forward passes keep 16 amplitudes per thread.
+static bool wide_forward() {
+  const char* v = std::getenv("VQC_JIT_WIDE");
+  return !(v && *v && std::atoi(v) == 0);
+}
 
 template <class R, int M, bool ADJ>
 static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
@@ -893,28 +900,49 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   const int n = h->nq;
   SerialPlan sp;
   const bool packed = use_packed(h);
-  serialize_plan<R, M, ADJ>(n, h->dtype, passes, sp, accs, packed);
+  // wide compiled forward passes: 32 amplitudes per thread, four free register
+  // bits per stage (fewer stages and barriers); the generic kernels take 16
+  int rb = (!ADJ && packed && use_jit(h) && wide_forward()) ? kWideRegBits : kRegBits;
+  const size_t accs0 = accs ? accs->size() : 0;
+  serialize_plan<R, M, ADJ>(n, h->dtype, passes, sp, accs, packed, rb);
   note_plan(ADJ, passes);
-  const std::vector<PassLoc>& locs = sp.locs;
-  const size_t pool_off = sp.pool_off;
   // run-time specialised kernels (FP32), one per pass structure
   std::vector<const void*> jk(passes.size(), nullptr);
   if constexpr (std::is_same<R, float>::value) {
     if (packed && use_jit(h)) {
-      std::vector<JitPassRef> refs(passes.size());
-      for (size_t pi = 0; pi < passes.size(); ++pi)
-        if (!locs[pi].standalone)
-          refs[pi] = JitPassRef{(const DevStageF*)(sp.buf.data() + locs[pi].stages), locs[pi].shape.nstages,
-                                (const DevOp*)(sp.buf.data() + locs[pi].ops), locs[pi].shape.npool};
-      jit_pass_kernels(M, ADJ, refs, jk);
+      auto compile = [&]() {
+        std::vector<JitPassRef> refs(passes.size());
+        for (size_t pi = 0; pi < passes.size(); ++pi)
+          if (!sp.locs[pi].standalone)
+            refs[pi] = JitPassRef{(const DevStageF*)(sp.buf.data() + sp.locs[pi].stages), sp.locs[pi].shape.nstages,
+                                  (const DevOp*)(sp.buf.data() + sp.locs[pi].ops), sp.locs[pi].shape.npool};
+        jit_pass_kernels(M, ADJ, refs, jk, false, true, rb);
+      };
+      compile();
+      if (rb != kRegBits) {
+        // a wide pass without a kernel (beyond the parameter space, or a failed
+        // compile) has no generic kernel: plan the whole sweep at 16 amplitudes
+        bool missing = false;
+        for (size_t pi = 0; pi < passes.size(); ++pi) missing = missing || (!sp.locs[pi].standalone && !jk[pi]);
+        if (missing) {
+          rb = kRegBits;
+          sp = SerialPlan();
+          if (accs) accs->resize(accs0);
+          serialize_plan<R, M, ADJ>(n, h->dtype, passes, sp, accs, packed, rb);
+          jk.assign(passes.size(), nullptr);
+          compile();
+        }
+      }
     }
   }
+  const std::vector<PassLoc>& locs = sp.locs;
+  const size_t pool_off = sp.pool_off;
   std::vector<int> grids(passes.size(), 0);
   for (size_t pi = 0; pi < passes.size(); ++pi) {
     if (locs[pi].standalone) continue;
     int g = 0;
     if constexpr (std::is_same<R, float>::value)
-      if (jk[pi]) g = jit_grid<M, ADJ>(h->device, jk[pi], locs[pi].shape);
+      if (jk[pi]) g = jit_grid<M, ADJ>(h->device, jk[pi], locs[pi].shape, rb);
     if (!g) g = tile_grid<R, M, ADJ>(h->device, locs[pi].shape);
     grids[pi] = (int)std::min<int64_t>(g, locs[pi].ntiles);
   }
@@ -959,7 +987,7 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
       if constexpr (std::is_same<R, float>::value)
         if ((rc = launch_tile_jit<M, ADJ>(h, jk[pi], psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape,
                                           sp.buf.data() + pool_off + locs[pi].pool_begin * sizeof(float2),
-                                          2.0 * locs[pi].fma_ops)))
+                                          2.0 * locs[pi].fma_ops, rb)))
           return rc;
     } else if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape,
                                             2.0 * locs[pi].fma_ops))) {

@@ -130,7 +130,7 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o, const char* cx) {
   os << "    { const DevOp* op = x.ops + " << o << ";\n";
   if (gctl) os << "      if ((x.base & op->gmask) == op->gval) {\n";
   if (type == kOpU1) {
-    const int tb = (code >> 4) & 3, rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = acc_kind_of(code);
+    const int tb = op_r0(code), rctl = (code >> 16) & 7, form = (code >> 11) & 7, kind = acc_kind_of(code);
     const int cb = rctl == 0 ? -1 : rctl - 1;
     os << "      const u64* c = " << cx << " + " << op.mat << ";\n";
     if (ctl) os << "      const bool run = (tthr & op->cmask) == op->cval;\n";
@@ -149,7 +149,7 @@ void emit_op(std::ostringstream& os, const DevOp& op, int o, const char* cx) {
     os << "      }\n";
     if (acc) os << "      " << ((kind & kAccAH) ? "flush4" : "flush8") << "(s8, x.sacc, op->slot, NW);\n";
   } else if (type == kOpU2) {
-    const int ja = (code >> 4) & 3, jb = (code >> 6) & 3;
+    const int ja = op_r0(code), jb = op_r1(code);
     if (ctl) os << "      if ((tthr & op->cmask) == op->cval)\n";
     os << "      u2_op<" << ja << ", " << jb << ", ADJ>(v, w, reinterpret_cast<const float2*>(" << cx << " + " << op.mat
        << "), (uint32_t)op->rmask);\n";
@@ -190,40 +190,44 @@ bool jit_available() { return nvrtc().ok; }
 // instead of four, and one more barrier per tile, cost more than the copy
 // saves; the default already prefetches the next tile into L2).
 bool jit_async_fwd() { return env_int("VQC_JIT_ASYNC", 0) != 0; }
-size_t jit_extra_smem(bool adj, int M) {
-  return (!adj && jit_async_fwd() && env_int("VQC_JIT_BAKE", 1)) ? (size_t(1) << (M - 1)) * 16 : 0;
+size_t jit_extra_smem(bool adj, int M, int rb) {
+  return (!adj && rb == kRegBits && jit_async_fwd() && env_int("VQC_JIT_BAKE", 1)) ? (size_t(1) << (M - 1)) * 16 : 0;
 }
 
 // Resident CTAs per SM the compiled kernels' registers are budgeted for:
 // 1024 threads for forward passes (64 registers), 768 when they hold a second
 // tile buffer (85 registers: their shared memory admits three 256-thread CTAs
-// anyway), 512 for the reverse sweep (128 registers).
-int jit_min_blocks(bool adj, int M) {
-  const int nt = 1 << (M - kRegBits);
+// anyway), 512 for the reverse sweep (128 registers); the wide forward passes
+// (32 amplitudes per thread) 640 (five 128-thread CTAs, 96 registers).
+int jit_min_blocks(bool adj, int M, int rb) {
+  const int nt = 1 << (M - rb);
   if (adj) return env_int("VQC_JIT_MINB_ADJ", 512 / nt);
+  if (rb != kRegBits) return std::max(1, env_int("VQC_JIT_MINB_WIDE", 640 / nt));
   return env_int("VQC_JIT_MINB_FWD", (jit_async_fwd() && env_int("VQC_JIT_BAKE", 1) ? 768 : 1024) / nt);
 }
 
-std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool, bool batch) {
+std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool, bool batch,
+                            int rb) {
   if (!batch && npool > kJitMaxCoef) return std::string();  // beyond the kernel-parameter space: interpreter
   std::ostringstream os;
-  const int NT = 1 << (M - kRegBits);
-  const bool bake = env_int("VQC_JIT_BAKE", 1) != 0;
-  const bool async = !batch && jit_extra_smem(adj, M) > 0;
+  const int NT = 1 << (M - rb), NP = 1 << (rb - 1);
+  // the wide passes exist only as compiled kernels with their offsets baked in
+  const bool bake = rb != kRegBits || env_int("VQC_JIT_BAKE", 1) != 0;
+  const bool async = !batch && jit_extra_smem(adj, M, rb) > 0;
   os << "#include \"tile_f32.cuh\"\n"
      << "using namespace vqc;\nusing namespace vqc::f32t;\n";
   if (!batch) {
     // the pass's matrix pool travels as a kernel parameter (constant bank,
     // read uniformly by the whole grid) instead of through shared memory
     os << "struct Coef { unsigned long long c[" << std::max(npool, 2) << "]; };\n"
-       << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M) << ")\n"
+       << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M, rb) << ")\n"
        << "vqc_pass(float2* psi, float2* lam, const DevPass* pass, const DevStageF* stages, const DevOp* ops,\n"
        << "         const float2* pool, double* partials, const __grid_constant__ Coef coef) {\n"
        << "  const int ncta = gridDim.x;\n";
   } else {
     // the serving loop: one request per blockIdx.y, each with its own state,
     // descriptors and coefficient pool (staged in shared memory)
-    os << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M) << ")\n"
+    os << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << jit_min_blocks(adj, M, rb) << ")\n"
        << "vqc_pass_batch(const TileItem* __restrict__ items) {\n"
        << "  const TileItem item = items[blockIdx.y];\n"
        << "  if ((int)blockIdx.x >= item.ncta) return;\n"
@@ -234,12 +238,13 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
        << "  double* partials = item.partials;\n";
   }
   os << "  constexpr int M = " << M << ";\n  constexpr bool ADJ = " << (adj ? "true" : "false") << ";\n"
-     << "  constexpr int NW = TileCtx<M, ADJ>::NW;\n"
+     << "  constexpr int RB = " << rb << ";\n"
+     << "  constexpr int NW = TileCtx<M, ADJ, RB>::NW;\n"
      << "  __shared__ DevPass P;\n  __shared__ uint64_t s_inc, s_base0;\n"
-     << "  TileCtx<M, ADJ> x;\n"
-     << "  tile_setup<M, ADJ" << (async ? ", 2" : "")
+     << "  TileCtx<M, ADJ, RB> x;\n"
+     << "  tile_setup<M, ADJ, " << (async ? 2 : 1)
      << ">(x, psi, lam, pass, stages, ops, pool, ncta, P, s_inc, s_base0, " << (batch ? "true" : "false") << ");\n"
-     << "  Pk v[8], w[8];\n";
+     << "  Pk v[" << NP << "], w[" << NP << "];\n";
   if (batch) os << "  const u64* C = reinterpret_cast<const u64*>(x.pool);\n";
   const char* cx = batch ? "C" : "coef.c";
   if (async) {
@@ -267,10 +272,10 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
       os << "};\n    stage_load_raw<M>(x, S, x.sp, v, swm);\n";
     } else if (bake) {
       // the stage's pair offsets as constants (they depend on the pass's qubits)
-      os << "    constexpr uint32_t swm[8] = {";
-      for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[s].swm[m] << "u";
-      os << "};\n    constexpr int64_t gdep[8] = {";
-      for (int m = 0; m < 8; ++m) os << (m ? ", " : "") << st[s].gdep[m] << "ll";
+      os << "    constexpr uint32_t swm[" << NP << "] = {";
+      for (int m = 0; m < NP; ++m) os << (m ? ", " : "") << st[s].swm[m] << "u";
+      os << "};\n    constexpr int64_t gdep[" << NP << "] = {";
+      for (int m = 0; m < NP; ++m) os << (m ? ", " : "") << st[s].gdep[m] << "ll";
       os << "};\n    stage_load_k<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w, swm, gdep);\n";
     } else {
       os << "    stage_load<M, ADJ>(x, S, " << (s == 0 ? "true" : "false") << ", v, w);\n";
@@ -397,11 +402,11 @@ std::set<std::pair<uint64_t, uint64_t>>& inflight() {
 }
 
 int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out, bool batch,
-                     bool compile) {
+                     bool compile, int rb) {
   out.assign(refs.size(), nullptr);
   if (!jit_available()) return VQC_OK;
-  const int flags[6] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M), M,
-                        batch ? 0 : (int)jit_extra_smem(adj, M), batch ? 1 : 0};
+  const int flags[7] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M, rb), M,
+                        batch ? 0 : (int)jit_extra_smem(adj, M, rb), batch ? 1 : 0, rb};
   std::vector<std::pair<uint64_t, uint64_t>> keys(refs.size());
   std::vector<size_t> miss;
   {
@@ -439,7 +444,7 @@ int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::
   std::vector<std::string> srcs(miss.size());
   for (size_t k = 0; k < miss.size(); ++k) {
     const JitPassRef& r = refs[miss[k]];
-    srcs[k] = jit_pass_source(M, adj, r.stages, r.nstages, r.ops, r.npool, batch);
+    srcs[k] = jit_pass_source(M, adj, r.stages, r.nstages, r.ops, r.npool, batch, rb);
   }
   std::vector<const void*> ks;
   int rc = jit_kernels(srcs, ks, batch ? "vqc_pass_batch" : "vqc_pass");

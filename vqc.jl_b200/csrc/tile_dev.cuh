@@ -44,25 +44,27 @@ struct alignas(16) DevStage {
 };
 
 // A stage of the FP32 (packed) tile body: tile bit 0 is always a register
-// bit (the lane bit inside each float4 pair), plus three free register bits.
+// bit (the lane bit inside each float4 pair), plus three free register bits
+// (16 amplitudes per thread), or four in the wide forward passes (32).
 // Per-thread quantities are split into two tables indexed by the thread
 // index's low and high nibble (thread bits are at most 8).
+constexpr int kWideRegBits = 5;  // wide compiled forward passes: 32 amplitudes per thread
 struct alignas(16) DevStageF {
-  int64_t gdep[8];       // global amplitude offset of register pair m (lane 0)
+  int64_t gdep[16];      // global amplitude offset of register pair m (lane 0)
   int64_t gthr[2][16];   // global offset of the thread's tile bits: [0][tid & 15] + [1][tid >> 4]
   uint32_t thr[2][16];   // tile index of the thread's bits: [0][tid & 15] | [1][tid >> 4]
   uint32_t swt[2][16];   // swizzled pair index of the thread's bits: [0][..] ^ [1][..]
-  uint32_t swm[8];       // swizzled pair index of register pair m
-  uint32_t dep[16];      // tile index of register amplitude j = lane + 2m
+  uint32_t swm[16];      // swizzled pair index of register pair m
+  uint32_t dep[32];      // tile index of register amplitude j = lane + 2m
   int32_t op_begin, op_end, pad0, pad1;
 };
 
 // code: bits 0-3 op type, 4-5 r0, 6-7 r1, 8 tile-bit controls, 9 non-tile
-// controls, 10 accumulate.  The first 16 bytes are read as one vector load.
-// In the FP32 body, r0/r1 are j-bits (0 = lane bit, 1..3 = free register
-// bits), cmask/cval hold only the controls on thread bits, and the controls
-// on register bits are bits 16-18 (0: none, 1..4: one control on j-bit
-// value-1 at |1>, 7: the amplitudes enabled in rmask).
+// controls, 10 accumulate, 20-21 the third bits of r0 / r1.  The first 16 bytes are read as one vector load.
+// In the FP32 body, r0/r1 are j-bits (0 = lane bit, 1..3 or 1..4 = free
+// register bits), cmask/cval hold only the controls on thread bits, and the
+// controls on register bits are bits 16-18 (0: none, 1..5: one control on
+// j-bit value-1 at |1>, 7: the amplitudes enabled in rmask).
 struct alignas(16) DevOp {
   int32_t code;
   int32_t mat;     // pool offset (complex elements)
@@ -75,6 +77,13 @@ struct alignas(16) DevOp {
   int32_t rmask;    // FP32 body: register amplitudes (pair representatives) the controls enable
 };
 constexpr int kCodeCtl = 1 << 8, kCodeGCtl = 1 << 9, kCodeAcc = 1 << 10;
+// r0 / r1 as 3-bit j-bits (the wide FP32 body has j-bits 0..4): bits 4-5 and
+// 6-7 hold the low two bits, bits 20 and 21 the third.
+__host__ __device__ constexpr int op_r0(int code) { return ((code >> 4) & 3) | (((code >> 20) & 1) << 2); }
+__host__ __device__ constexpr int op_r1(int code) { return ((code >> 6) & 3) | (((code >> 21) & 1) << 2); }
+__host__ __device__ constexpr int op_r_bits(int r0, int r1) {
+  return ((r0 & 3) << 4) | ((r1 & 3) << 6) | ((r0 >> 2) << 20) | ((r1 >> 2) << 21);
+}
 // bits 11-13: one-qubit matrix form; bits 14-15: reduced-matrix entries
 // accumulated; bits 16-18: register control; bit 19: anti-Hermitian projection
 constexpr int kCodeAH = 1 << 19;

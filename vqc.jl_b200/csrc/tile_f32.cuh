@@ -56,12 +56,14 @@ struct Pk {
   u64 r, i;
 };
 
-// amplitude j = lane + 2m of the thread's 16 (j compile-time after unrolling)
-__device__ __forceinline__ float2 amp(const Pk (&v)[8], int j) {
+// amplitude j = lane + 2m of the thread's 2 NP (j compile-time after unrolling)
+template <int NP>
+__device__ __forceinline__ float2 amp(const Pk (&v)[NP], int j) {
   const Pk& q = v[j >> 1];
   return (j & 1) ? make_float2(hi(q.r), hi(q.i)) : make_float2(lo(q.r), lo(q.i));
 }
-__device__ __forceinline__ void set_amp(Pk (&v)[8], int j, float2 a) {
+template <int NP>
+__device__ __forceinline__ void set_amp(Pk (&v)[NP], int j, float2 a) {
   Pk& q = v[j >> 1];
   if (j & 1) {
     q.r = mk(lo(q.r), a.x);
@@ -209,13 +211,14 @@ __device__ __forceinline__ void lane_apply(Pk& V, const u64* c) {
   }
 }
 
-// j-bit layout of the 16 amplitudes: bit 0 = lane, bits 1..3 = free slots.
-// TB: target j-bit.  CB: single register control (j-bit, at |1>), or -1.
-template <int TB, int CB, int FORM, bool ADJ>
-__device__ __forceinline__ void u1_static(Pk (&v)[8], Pk (&w)[8], const u64* c) {
+// j-bit layout of the 2 NP amplitudes: bit 0 = lane, bits 1.. = free slots
+// (NP = 8: three, NP = 16: four).  TB: target j-bit.  CB: single register
+// control (j-bit, at |1>), or -1.
+template <int TB, int CB, int FORM, bool ADJ, int NP>
+__device__ __forceinline__ void u1_static(Pk (&v)[NP], Pk (&w)[NP], const u64* c) {
   if constexpr (TB == 0) {
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < NP; ++m) {
       if (CB > 0 && !((m >> (CB - 1)) & 1)) continue;
       lane_apply<FORM>(v[m], c);
       if (ADJ) lane_apply<FORM, true>(w[m], c);
@@ -223,7 +226,7 @@ __device__ __forceinline__ void u1_static(Pk (&v)[8], Pk (&w)[8], const u64* c) 
   } else {
     constexpr int T = TB - 1;
 #pragma unroll
-    for (int g = 0; g < 4; ++g) {
+    for (int g = 0; g < NP / 2; ++g) {
       const int m0 = ((g >> T) << (T + 1)) | (g & ((1 << T) - 1)), m1 = m0 | (1 << T);
       if (CB > 0 && !((m0 >> (CB - 1)) & 1)) continue;
       if (CB == 0) {  // lane control: lane 1 only
@@ -239,11 +242,11 @@ __device__ __forceinline__ void u1_static(Pk (&v)[8], Pk (&w)[8], const u64* c) 
 
 // Register controls given as a mask over the pair representatives (bit j set:
 // amplitude j, target bit clear, satisfies the register controls).
-template <int TB, int FORM, bool ADJ>
-__device__ __forceinline__ void u1_masked(Pk (&v)[8], Pk (&w)[8], const u64* c, uint32_t rmask) {
+template <int TB, int FORM, bool ADJ, int NP>
+__device__ __forceinline__ void u1_masked(Pk (&v)[NP], Pk (&w)[NP], const u64* c, uint32_t rmask) {
   if constexpr (TB == 0) {
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < NP; ++m) {
       if (!((rmask >> (2 * m)) & 1)) continue;
       lane_apply<FORM>(v[m], c);
       if (ADJ) lane_apply<FORM, true>(w[m], c);
@@ -251,7 +254,7 @@ __device__ __forceinline__ void u1_masked(Pk (&v)[8], Pk (&w)[8], const u64* c, 
   } else {
     constexpr int T = TB - 1;
 #pragma unroll
-    for (int g = 0; g < 4; ++g) {
+    for (int g = 0; g < NP / 2; ++g) {
       const int m0 = ((g >> T) << (T + 1)) | (g & ((1 << T) - 1)), m1 = m0 | (1 << T);
       if ((rmask >> (2 * m0)) & 1) {
         scalar_apply<FORM, 0>(v[m0], v[m1], c);
@@ -589,10 +592,10 @@ __device__ __forceinline__ void u1_target(int rctl, int form, bool acc, int kind
 
 // Two target j-bits JA < JB: dense 4x4 (bit 0 <-> JA) on each quad whose base
 // amplitude is enabled in rmask.
-template <int JA, int JB, bool ADJ>
-__device__ __forceinline__ void u2_op(Pk (&v)[8], Pk (&w)[8], const float2* U, uint32_t rmask) {
+template <int JA, int JB, bool ADJ, int NP>
+__device__ __forceinline__ void u2_op(Pk (&v)[NP], Pk (&w)[NP], const float2* U, uint32_t rmask) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < NP / 2; ++q) {
     int j = q;
     j = ((j >> JA) << (JA + 1)) | (j & ((1 << JA) - 1));
     j = ((j >> JB) << (JB + 1)) | (j & ((1 << JB) - 1));
@@ -600,7 +603,7 @@ __device__ __forceinline__ void u2_op(Pk (&v)[8], Pk (&w)[8], const float2* U, u
     const int idx[4] = {j, j | (1 << JA), j | (1 << JB), j | (1 << JA) | (1 << JB)};
 #pragma unroll
     for (int st = 0; st < (ADJ ? 2 : 1); ++st) {
-      Pk(&s)[8] = st ? w : v;
+      Pk(&s)[NP] = st ? w : v;
       float2 x[4], o[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) x[i] = amp(s, idx[i]);
@@ -635,8 +638,8 @@ __device__ __forceinline__ void u2_dispatch(int ja, int jb, Pk (&v)[8], Pk (&w)[
 // ----------------------------------------------------------------------------- diagonal ops
 // Diagonal (phase) op: phase index from the op's qubits, tile bits per
 // amplitude and non-tile qubits per tile.
-template <bool ADJ>
-__device__ __forceinline__ void diag_op(Pk (&v)[8], Pk (&w)[8], const DevOp* op, const float2* c, uint32_t tthr,
+template <bool ADJ, int NP>
+__device__ __forceinline__ void diag_op(Pk (&v)[NP], Pk (&w)[NP], const DevOp* op, const float2* c, uint32_t tthr,
                                         const uint32_t* dep, uint64_t base) {
   const int nd = op->nd;
   uint32_t gidx = 0;
@@ -647,7 +650,7 @@ __device__ __forceinline__ void diag_op(Pk (&v)[8], Pk (&w)[8], const DevOp* op,
     if (i < nd && db[i] < 0) gidx |= (uint32_t)((base >> op->dglob[i]) & 1) << i;
   }
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
+  for (int j = 0; j < 2 * NP; ++j) {
     const uint32_t t = tthr | dep[j];
     uint32_t idx = gidx;
 #pragma unroll
@@ -691,9 +694,9 @@ __device__ __forceinline__ void accd_op(const Pk (&v)[8], const Pk (&w)[8], cons
 // Per-CTA context of a pass: the state pointers, the staged descriptors in
 // shared memory, and the tile counter in the deposited (non-tile bit) space,
 // base(t + ncta) = ((base | ~mask) + inc) & mask.
-template <int M, bool ADJ>
+template <int M, bool ADJ, int RB = kRegBits>
 struct TileCtx {
-  static constexpr int NT = 1 << (M - kRegBits), NW = NT / 32, NPAIR = 1 << (M - 1);
+  static constexpr int NT = 1 << (M - RB), NW = NT / 32, NPAIR = 1 << (M - 1);
   float2* psi;
   float2* lam;
   ulonglong2* sp;
@@ -712,11 +715,11 @@ struct TileCtx {
 // the tile counter.  Every thread of the CTA calls it.  NBUF = 2 puts a
 // second tile buffer in front of the usual layout (the asynchronous forward
 // passes copy the next tile into it while the current one is computed).
-template <int M, bool ADJ, int NBUF = 1>
-__device__ __forceinline__ void tile_setup(TileCtx<M, ADJ>& x, float2* psi, float2* lam, const DevPass* pass,
+template <int M, bool ADJ, int NBUF = 1, int RB = kRegBits>
+__device__ __forceinline__ void tile_setup(TileCtx<M, ADJ, RB>& x, float2* psi, float2* lam, const DevPass* pass,
                                            const DevStageF* stages, const DevOp* ops, const float2* pool, int ncta,
                                            DevPass& P, uint64_t& s_inc, uint64_t& s_base0, bool stage_pool = true) {
-  constexpr int NT = TileCtx<M, ADJ>::NT, NW = TileCtx<M, ADJ>::NW, NPAIR = TileCtx<M, ADJ>::NPAIR;
+  constexpr int NT = TileCtx<M, ADJ, RB>::NT, NW = TileCtx<M, ADJ, RB>::NW, NPAIR = TileCtx<M, ADJ, RB>::NPAIR;
   extern __shared__ __align__(16) unsigned char smem_all[];
   unsigned char* smem = smem_all + (NBUF - 1) * (unsigned long long)NPAIR * 16;
   if (threadIdx.x == 0) P = *pass;
@@ -836,13 +839,15 @@ __device__ __forceinline__ void stage_store(const TileCtx<M, ADJ>& x, const DevS
 }
 // The same with the stage's pair offsets as compile-time constants (the
 // compiled pass kernels): no dependent descriptor loads before the data.
-template <int M, bool ADJ>
-__device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ>& x, const DevStageF* S, bool first, Pk (&v)[8],
-                                             Pk (&w)[8], const uint32_t (&swm)[8], const int64_t (&gdep)[8]) {
+template <int M, bool ADJ, int RB, int NP>
+__device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ, RB>& x, const DevStageF* S, bool first,
+                                             Pk (&v)[NP], Pk (&w)[NP], const uint32_t (&swm)[NP],
+                                             const int64_t (&gdep)[NP]) {
+  static_assert(NP == (1 << (RB - 1)), "register pairs");
   if (first) {
     const int64_t g0 = (int64_t)x.base + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < NP; ++m) {
       const int64_t gi = g0 + gdep[m];
       if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       const float4 t = *reinterpret_cast<const float4*>(x.psi + gi);
@@ -857,9 +862,9 @@ __device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ>& x, const Dev
   } else {
     const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < NP; ++m) {
       const uint32_t a = sw ^ swm[m];
-      if (!VQC_DCHECK(a, (TileCtx<M, ADJ>::NPAIR))) continue;
+      if (!VQC_DCHECK(a, (TileCtx<M, ADJ, RB>::NPAIR))) continue;
       const ulonglong2 t = x.sp[a];
       v[m].r = t.x;
       v[m].i = t.y;
@@ -871,14 +876,14 @@ __device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ>& x, const Dev
     }
   }
 }
-template <int M, bool ADJ>
-__device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const DevStageF* S, bool last,
-                                              const Pk (&v)[8], const Pk (&w)[8], const uint32_t (&swm)[8],
-                                              const int64_t (&gdep)[8]) {
+template <int M, bool ADJ, int RB, int NP>
+__device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ, RB>& x, const DevStageF* S, bool last,
+                                              const Pk (&v)[NP], const Pk (&w)[NP], const uint32_t (&swm)[NP],
+                                              const int64_t (&gdep)[NP]) {
   if (last) {
     const int64_t g0 = (int64_t)x.base + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < NP; ++m) {
       const int64_t gi = g0 + gdep[m];
       if (!VQC_DCHECK(gi + 1, x.P->ntiles << M)) continue;
       *reinterpret_cast<float4*>(x.psi + gi) = make_float4(lo(v[m].r), lo(v[m].i), hi(v[m].r), hi(v[m].i));
@@ -888,9 +893,9 @@ __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ>& x, const De
   } else {
     const uint32_t sw = S->swt[0][x.tlo] ^ S->swt[1][x.thi];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
+    for (int m = 0; m < NP; ++m) {
       const uint32_t a = sw ^ swm[m];
-      if (!VQC_DCHECK(a, (TileCtx<M, ADJ>::NPAIR))) continue;
+      if (!VQC_DCHECK(a, (TileCtx<M, ADJ, RB>::NPAIR))) continue;
       x.sp[a] = make_ulonglong2(v[m].r, v[m].i);
       if (ADJ) x.sl[a] = make_ulonglong2(w[m].r, w[m].i);
     }
@@ -949,26 +954,26 @@ __device__ __forceinline__ void stage_load_raw(const TileCtx<M, false>& x, const
 
 // L2 prefetch of the next tile's first-stage pairs (no shared memory, no
 // registers held): the next tile's loads then come from L2.
-template <int M, bool ADJ>
-__device__ __forceinline__ void prefetch_next_l2(const TileCtx<M, ADJ>& x, const DevStageF* S, uint64_t s_inc,
-                                                 const int64_t (&gdep)[8]) {
+template <int M, bool ADJ, int RB, int NP>
+__device__ __forceinline__ void prefetch_next_l2(const TileCtx<M, ADJ, RB>& x, const DevStageF* S, uint64_t s_inc,
+                                                 const int64_t (&gdep)[NP]) {
   const uint64_t next = ((x.base | ~x.P->nontile_mask) + s_inc) & x.P->nontile_mask;
   const int64_t g0 = (int64_t)next + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
+  for (int m = 0; m < NP; ++m) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(x.psi + g0 + gdep[m]));
     if (ADJ) asm volatile("prefetch.global.L2 [%0];" ::"l"(x.lam + g0 + gdep[m]));
   }
 }
 
-template <int M, bool ADJ>
-__device__ __forceinline__ void tile_next(TileCtx<M, ADJ>& x, uint64_t s_inc) {
+template <int M, bool ADJ, int RB>
+__device__ __forceinline__ void tile_next(TileCtx<M, ADJ, RB>& x, uint64_t s_inc) {
   x.base = ((x.base | ~x.P->nontile_mask) + s_inc) & x.P->nontile_mask;
 }
 // Per-warp slot rows -> this CTA's partials row (fixed order).
-template <int M, bool ADJ>
-__device__ __forceinline__ void tile_finish(const TileCtx<M, ADJ>& x, double* partials) {
-  constexpr int NT = TileCtx<M, ADJ>::NT, NW = TileCtx<M, ADJ>::NW;
+template <int M, bool ADJ, int RB>
+__device__ __forceinline__ void tile_finish(const TileCtx<M, ADJ, RB>& x, double* partials) {
+  constexpr int NT = TileCtx<M, ADJ, RB>::NT, NW = TileCtx<M, ADJ, RB>::NW;
   const int nslots = ADJ ? x.P->nslots : 0;
   if (ADJ && nslots > 0) {
     __syncthreads();

@@ -128,15 +128,15 @@ struct ReqPlan {
 // Run-time specialised FP32 tile kernels (jit.cu).
 int jit_mode();        // 0 off, 1 on, 2 auto, 3 packed interpreter (VQC_JIT)
 bool jit_available();  // NVRTC could be loaded
-int jit_min_blocks(bool adj, int M);
+int jit_min_blocks(bool adj, int M, int rb = kRegBits);
 // Shared-memory bytes a compiled pass needs beyond pass_smem (the second tile
 // buffer of the asynchronous forward passes).
-size_t jit_extra_smem(bool adj, int M);
+size_t jit_extra_smem(bool adj, int M, int rb = kRegBits);
 // Source of a pass's kernel ("" when the pass is not compiled: its matrix
 // pool, passed as a kernel parameter, would exceed kJitMaxCoef entries).
 constexpr int kJitMaxCoef = 3800;
 std::string jit_pass_source(int M, bool adj, const DevStageF* stages, int nstages, const DevOp* ops, int npool,
-                            bool batch = false);
+                            bool batch = false, int rb = kRegBits);
 // Compiler threads jit_kernels may start from the calling thread (0: one per
 // host core).  A background compiler sets a few so the threads that plan and
 // launch keep their cores.
@@ -154,8 +154,10 @@ struct JitPassRef {
 // batch: the serving loop's kernels (vqc_pass_batch over an array of TileItems,
 // coefficients from each item's pool) instead of the single-state ones.
 // compile = false: look up only (a structure not compiled yet gives nullptr).
+// rb: register bits per thread of the passes' stage layout (kRegBits, or
+// kWideRegBits for wide forward passes).
 int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::vector<const void*>& out,
-                     bool batch = false, bool compile = true);
+                     bool batch = false, bool compile = true, int rb = kRegBits);
 
 // compiled: an FP32 packed plan with compiled batch kernels (fwd_k / adj_k)
 // when every pass has one already, else the classic plan for the generic
