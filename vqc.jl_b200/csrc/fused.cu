@@ -888,10 +888,13 @@ static bool use_jit(const vqc_state h) {
 // The packed FP32 plan layout: for the compiled passes, or forced with
 // VQC_JIT=interp (the packed interpreter, the compiled kernels' fallback).
 static bool use_packed(const vqc_state h) { return h->dtype == VQC_C64 && (use_jit(h) || jit_mode() == 3); }
-// VQC_JIT_WIDE=0: the compiled forward passes keep 16 amplitudes per thread.
+// VQC_JIT_WIDE=1: compiled forward passes with 32 amplitudes per thread (four
+// free register bits per stage: 3.0 instead of 3.8 stages per pass on the
+// headline circuit).  Off by default: NVRTC takes 15-140 s per such pass
+// (1-2 s at 16 amplitudes), in its optimizer, not in ptxas.
 static bool wide_forward() {
   const char* v = std::getenv("VQC_JIT_WIDE");
-  return !(v && *v && std::atoi(v) == 0);
+  return v && *v && std::atoi(v) != 0;
 }
 
 template <class R, int M, bool ADJ>
@@ -900,8 +903,8 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
   const int n = h->nq;
   SerialPlan sp;
   const bool packed = use_packed(h);
-  // wide compiled forward passes: 32 amplitudes per thread, four free register
-  // bits per stage (fewer stages and barriers); the generic kernels take 16
+  // wide compiled forward passes (VQC_JIT_WIDE=1): 32 amplitudes per thread,
+  // four free register bits per stage; the generic kernels take 16
   int rb = (!ADJ && packed && use_jit(h) && wide_forward()) ? kWideRegBits : kRegBits;
   const size_t accs0 = accs ? accs->size() : 0;
   serialize_plan<R, M, ADJ>(n, h->dtype, passes, sp, accs, packed, rb);
