@@ -999,16 +999,16 @@ constexpr size_t kPTJitMaxCoefBytes = 30000;  // kernel-parameter space
 
 static int parity64(uint64_t m) { return __builtin_popcountll(m) & 1; }
 
-// Block shape of the compiled passes: 256 threads, three CTAs per SM (a CTA
-// loading its tile overlaps the others' compute), or 512 threads, two CTAs
-// (VQC_PAULI_NT=512).
+// Block shape of the compiled passes: 512 threads, two CTAs per SM, or 256
+// threads, three CTAs (VQC_PAULI_NT=256; measured slower at 2^26 FP32
+// amplitudes: 1.09 against 0.965 ms per Pauli step).
 struct PTJitShape {
   int threads, per_sm;
 };
 static PTJitShape pt_jit_shape() {
   const char* v = std::getenv("VQC_PAULI_NT");
-  if (v && *v && std::atoi(v) == 512) return {512, 2};
-  return {256, 3};
+  if (v && *v && std::atoi(v) == 256) return {256, 3};
+  return {512, 2};
 }
 
 // Source of one compiled pass; coef receives the parameter values in the

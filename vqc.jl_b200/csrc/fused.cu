@@ -890,8 +890,10 @@ static bool use_jit(const vqc_state h) {
 static bool use_packed(const vqc_state h) { return h->dtype == VQC_C64 && (use_jit(h) || jit_mode() == 3); }
 // VQC_JIT_WIDE=1: compiled forward passes with 32 amplitudes per thread (four
 // free register bits per stage: 3.0 instead of 3.8 stages per pass on the
-// headline circuit).  Off by default: NVRTC takes 15-140 s per such pass
-// (1-2 s at 16 amplitudes), in its optimizer, not in ptxas.
+// headline circuit).  Off by default: measured slower at 2^26 amplitudes
+// (0.40 against 0.355 ms per pass: five 128-thread CTAs per SM at 96
+// registers, with spills), and NVRTC takes 15-140 s per such pass (1-2 s at
+// 16 amplitudes), in its optimizer, not in ptxas.
 static bool wide_forward() {
   const char* v = std::getenv("VQC_JIT_WIDE");
   return v && *v && std::atoi(v) != 0;
