@@ -182,6 +182,8 @@ int workspace(vqc_state h, int count, void** bufs);
 int enter(vqc_state h);
 // Grows h->opbuf to at least `bytes` and copies `src` into it (stream-ordered).
 int upload_ops(vqc_state h, const void* src, size_t bytes);
+int reserve_ops(vqc_state h, size_t bytes);
+int upload_ops_at(vqc_state h, size_t off, const void* src, size_t bytes);
 // Copies `n` reduced doubles from h->scr.result to h->h_result and waits.
 int fetch_result(vqc_state h, int n);
 }  // namespace vqc

@@ -30,6 +30,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <thread>
 #include <type_traits>
 
 #include "engine.h"
@@ -899,9 +900,21 @@ static bool wide_forward() {
   return v && *v && std::atoi(v) != 0;
 }
 
+// An upper bound of one pass's serialised bytes (serialize_plan): at most one
+// stage per op, two op records per op, 32 matrix entries (+ alignment) per op.
+template <class R>
+static size_t op_bytes_bound(const PlanPass& p) {
+  const size_t nops = p.ops.size() + 1;
+  return 3 * 16 + sizeof(DevPass) + nops * std::max(sizeof(DevStageF), sizeof(DevStage)) + 2 * nops * sizeof(DevOp) +
+         (34 * nops + 8) * sizeof(cplx<R>);
+}
+
+// op_used != nullptr: the pass descriptors go to the op buffer at op_off
+// (reserved by the caller) and *op_used receives their size, so that later
+// chunks of one sweep can be uploaded while these passes run.
 template <class R, int M, bool ADJ>
 static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& passes, const std::vector<GateSpec>& specs,
-                    std::vector<AccRef>* accs, double* rows_dev) {
+                    std::vector<AccRef>* accs, double* rows_dev, size_t op_off = 0, size_t* op_used = nullptr) {
   const int n = h->nq;
   SerialPlan sp;
   const bool packed = use_packed(h);
@@ -951,9 +964,10 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     if (!g) g = tile_grid<R, M, ADJ>(h->device, locs[pi].shape);
     grids[pi] = (int)std::min<int64_t>(g, locs[pi].ntiles);
   }
-  int rc = upload_ops(h, sp.buf.data(), sp.buf.size());
+  int rc = op_used ? upload_ops_at(h, op_off, sp.buf.data(), sp.buf.size()) : upload_ops(h, sp.buf.data(), sp.buf.size());
   if (rc) return rc;
-  const unsigned char* base = (const unsigned char*)h->opbuf;
+  if (op_used) *op_used = sp.buf.size();
+  const unsigned char* base = (const unsigned char*)h->opbuf + op_off;
   // partial sums scratch: one row of 8 doubles per (CTA, slot) of the largest pass
   size_t need = 0;
   for (size_t pi = 0; pi < passes.size(); ++pi)
@@ -1012,15 +1026,49 @@ template <class R, int M>
 static int forward_impl(vqc_state h, const vqc_gate* gates, int ngates, const double* mats) {
   std::vector<GateSpec> specs(ngates);
   std::vector<PItem> items(ngates);
-  for (int i = 0; i < ngates; ++i) {
-    int rc = analyze_gate(h->nq, gates[i].nq, gates[i].pos, mats + gates[i].mat, false, specs[i]);
-    if (rc) return rc;
-    items[i].gate = i;
-    items[i].standalone = !to_fop(specs[i], items[i].op);
-  }
+  // gate analysis, on up to four host threads for long circuits (it precedes
+  // the first launch: the device waits for it)
+  auto analyze = [&](int i0, int i1) {
+    for (int i = i0; i < i1; ++i) {
+      if (analyze_gate(h->nq, gates[i].nq, gates[i].pos, mats + gates[i].mat, false, specs[i])) return i;
+      items[i].gate = i;
+      items[i].standalone = !to_fop(specs[i], items[i].op);
+    }
+    return -1;
+  };
+  const int nth = ngates >= 1024 ? (int)std::min(4u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+  std::vector<int> bad(nth, -1);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nth; ++t)
+    pool.emplace_back([&, t] { bad[t] = analyze((int)((int64_t)ngates * t / nth), (int)((int64_t)ngates * (t + 1) / nth)); });
+  bad[0] = analyze(0, (int)((int64_t)ngates / nth));
+  for (auto& th : pool) th.join();
+  for (int t = 0; t < nth; ++t)
+    if (bad[t] >= 0)  // again on this thread, for its error message
+      return analyze_gate(h->nq, gates[bad[t]].nq, gates[bad[t]].pos, mats + gates[bad[t]].mat, false, specs[bad[t]]);
   std::vector<PlanPass> passes;
   plan_passes(h->nq, tile_config(h->dtype, h->nq), false, items, passes);
-  return run_plan<R, M, false>(h, h->d, nullptr, passes, specs, nullptr, nullptr);
+  const char* pc = std::getenv("VQC_PLAN_CHUNKS");  // 0: one serialisation for the whole sweep
+  if (passes.size() < 4 || (pc && *pc && std::atoi(pc) == 0))
+    return run_plan<R, M, false>(h, h->d, nullptr, passes, specs, nullptr, nullptr);
+  // Serialised and launched in chunks of 1, 2, 4, ... passes: the host plans
+  // the next chunk while the device runs the previous ones, instead of the
+  // device waiting for the whole sweep's descriptors (about 1.5 ms for 2,000
+  // gates).  Each chunk's descriptors get their own region of the op buffer.
+  size_t bound = 256;
+  for (const PlanPass& p : passes) bound += op_bytes_bound<R>(p);
+  int rc = reserve_ops(h, bound);
+  if (rc) return rc;
+  size_t off = 0, take = 1;
+  for (size_t first = 0; first < passes.size(); first += take, take *= 2) {
+    const size_t last = std::min(passes.size(), first + take);
+    std::vector<PlanPass> chunk(std::make_move_iterator(passes.begin() + first),
+                                std::make_move_iterator(passes.begin() + last));
+    size_t used = 0;
+    if ((rc = run_plan<R, M, false>(h, h->d, nullptr, chunk, specs, nullptr, nullptr, off, &used))) return rc;
+    off = (off + used + 255) & ~size_t(255);
+  }
+  return VQC_OK;
 }
 
 int apply_circuit_fused(vqc_state h, const vqc_gate* gates, int ngates, const double* mats) {

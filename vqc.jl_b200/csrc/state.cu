@@ -67,6 +67,33 @@ int upload_ops(vqc_state h, const void* src, size_t bytes) {
   return VQC_OK;
 }
 
+// The op buffer holds at least `bytes` (a larger buffer replaces it after the
+// stream has drained: call before uploading anything the coming launches read).
+int reserve_ops(vqc_state h, size_t bytes) {
+  if (bytes <= h->opbuf_bytes) return VQC_OK;
+  if (h->opbuf) {
+    VQC_CK(cudaStreamSynchronize(h->stream));
+    VQC_CK(cudaFree(h->opbuf));
+    h->opbuf = nullptr;
+    h->opbuf_bytes = 0;
+  }
+  size_t cap = 1 << 16;
+  while (cap < bytes) cap <<= 1;
+  VQC_CK(cudaMalloc(&h->opbuf, cap));
+  h->opbuf_bytes = cap;
+  return VQC_OK;
+}
+
+// Upload into the op buffer at byte offset `off` (reserved with reserve_ops);
+// stream-ordered like upload_ops, so launches queued before it keep reading
+// the bytes they were given elsewhere in the buffer.
+int upload_ops_at(vqc_state h, size_t off, const void* src, size_t bytes) {
+  if (bytes == 0) return VQC_OK;
+  if (off + bytes > h->opbuf_bytes) return fail(VQC_ERR_ARG, "internal: op upload beyond the reserved buffer");
+  VQC_CK(cudaMemcpyAsync((unsigned char*)h->opbuf + off, src, bytes, cudaMemcpyHostToDevice, h->stream));
+  return VQC_OK;
+}
+
 int stream_after(vqc_state dst, vqc_state src) {
   if (src == dst || src->stream == dst->stream) return VQC_OK;
   cudaEvent_t ev;
