@@ -43,25 +43,10 @@ namespace vqc {
 
 // The tile kernels themselves live in tile_kernels_impl.cuh (tile_inst_*.cu).
 
-// Sums the per-CTA partials over the grid in a fixed order: block = slot.
-__global__ void __launch_bounds__(256) k_reduce_slots(const double* __restrict__ partials, int nblocks, int nslots,
-                                                      int row0, double* __restrict__ out) {
-  __shared__ double sm[8][8];
-  const int slot = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int val = 0; val < 8; ++val) {
-    double s = 0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[((size_t)b * nslots + slot) * 8 + val];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) sm[warp][val] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x < 8) {
-    double s = 0;
-    for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) s += sm[wp][threadIdx.x];
-    out[(size_t)(row0 + slot) * 8 + threadIdx.x] = s;
-  }
-}
+// Sums the per-CTA partials of many passes over their grids in a fixed order:
+// one item per pass (blockIdx.y), block x = slot (defined with the serving
+// support below).
+__global__ void __launch_bounds__(256) k_reduce_slots_batch(const RedItem* __restrict__ items);
 
 // ----------------------------------------------------------------------------- host planner
 // A gate in planner form: one op, or "standalone" (kept as a GateSpec).
@@ -964,15 +949,18 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     if (!g) g = tile_grid<R, M, ADJ>(h->device, locs[pi].shape);
     grids[pi] = (int)std::min<int64_t>(g, locs[pi].ntiles);
   }
-  int rc = op_used ? upload_ops_at(h, op_off, sp.buf.data(), sp.buf.size()) : upload_ops(h, sp.buf.data(), sp.buf.size());
-  if (rc) return rc;
-  if (op_used) *op_used = sp.buf.size();
-  const unsigned char* base = (const unsigned char*)h->opbuf + op_off;
-  // partial sums scratch: one row of 8 doubles per (CTA, slot) of the largest pass
+  // partial sums scratch: one row of 8 doubles per (CTA, slot) of every pass,
+  // summed over the CTAs by one launch after the sweep (the same fixed order
+  // per slot as a reduction after each pass)
+  std::vector<size_t> poff(passes.size(), 0);
   size_t need = 0;
+  int max_slots = 0;
   for (size_t pi = 0; pi < passes.size(); ++pi)
-    if (!locs[pi].standalone && locs[pi].nslots > 0)
-      need = std::max(need, (size_t)grids[pi] * locs[pi].nslots * 8 * sizeof(double));
+    if (!locs[pi].standalone && locs[pi].nslots > 0) {
+      poff[pi] = need / sizeof(double);
+      need += (size_t)grids[pi] * locs[pi].nslots * 8 * sizeof(double);
+      max_slots = std::max(max_slots, locs[pi].nslots);
+    }
   double* partials = nullptr;
   if (ADJ && need > 0) {
     if (need > h->fused_scratch_bytes) {
@@ -986,6 +974,22 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
     }
     partials = (double*)h->fused_scratch;
   }
+  // the reduction items travel with the pass descriptors
+  size_t red_off = 0, nred = 0;
+  if (ADJ && need > 0) {
+    std::vector<RedItem> red;
+    for (size_t pi = 0; pi < passes.size(); ++pi)
+      if (!locs[pi].standalone && locs[pi].nslots > 0)
+        red.push_back(RedItem{partials + poff[pi], grids[pi], locs[pi].nslots, rows_dev + (size_t)locs[pi].row0 * 8});
+    red_off = (sp.buf.size() + 15) & ~size_t(15);
+    nred = red.size();
+    sp.buf.resize(red_off + sizeof(RedItem) * nred);
+    std::memcpy(sp.buf.data() + red_off, red.data(), sizeof(RedItem) * nred);
+  }
+  int rc = op_used ? upload_ops_at(h, op_off, sp.buf.data(), sp.buf.size()) : upload_ops(h, sp.buf.data(), sp.buf.size());
+  if (rc) return rc;
+  if (op_used) *op_used = sp.buf.size();
+  const unsigned char* base = (const unsigned char*)h->opbuf + op_off;
   for (size_t pi = 0; pi < passes.size(); ++pi) {
     if (locs[pi].standalone) {
       const GateSpec& gs = specs[locs[pi].gate];
@@ -996,26 +1000,27 @@ static int run_plan(vqc_state h, void* psi, void* lam, std::vector<PlanPass>& pa
       }
       continue;
     }
-    const int nslots = locs[pi].nslots;
     const int grid = grids[pi];
+    double* pp = partials ? partials + poff[pi] : nullptr;
     const DevPass* dp = (const DevPass*)(base + locs[pi].pass);
     const void* ds = (const void*)(base + locs[pi].stages);
     const DevOp* dops = (const DevOp*)(base + locs[pi].ops);
     const void* dpool = base + pool_off + locs[pi].pool_begin * sizeof(cplx<R>);
     if (jk[pi]) {
       if constexpr (std::is_same<R, float>::value)
-        if ((rc = launch_tile_jit<M, ADJ>(h, jk[pi], psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape,
+        if ((rc = launch_tile_jit<M, ADJ>(h, jk[pi], psi, lam, dp, ds, dops, dpool, pp, grid,
+                                          locs[pi].shape,
                                           sp.buf.data() + pool_off + locs[pi].pool_begin * sizeof(float2),
                                           2.0 * locs[pi].fma_ops, rb)))
           return rc;
-    } else if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, dp, ds, dops, dpool, partials, grid, locs[pi].shape,
+    } else if ((rc = launch_tile<R, M, ADJ>(h, psi, lam, dp, ds, dops, dpool, pp, grid, locs[pi].shape,
                                             2.0 * locs[pi].fma_ops))) {
       return rc;
     }
-    if (ADJ && nslots > 0) {
-      k_reduce_slots<<<nslots, 256, 0, h->stream>>>(partials, grid, nslots, locs[pi].row0, rows_dev);
-      VQC_CK(cudaGetLastError());
-    }
+  }
+  if (nred > 0) {
+    k_reduce_slots_batch<<<dim3(max_slots, (unsigned)nred), 256, 0, h->stream>>>((const RedItem*)(base + red_off));
+    VQC_CK(cudaGetLastError());
   }
   return VQC_OK;
 }
