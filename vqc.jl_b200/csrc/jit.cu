@@ -206,6 +206,15 @@ int jit_min_blocks(bool adj, int M, int rb) {
   return env_int("VQC_JIT_MINB_FWD", (jit_async_fwd() && env_int("VQC_JIT_BAKE", 1) ? 768 : 1024) / nt);
 }
 
+// Tile bits of the warp index in a stage's thread layout (thread bit j is the
+// stage's j-th tile bit outside the register set; the warp index is thread
+// bits 5 and up).
+static uint32_t warp_tile_bits(const DevStageF& st, int thread_bits) {
+  uint32_t m = 0;
+  for (int j = 5; j < thread_bits; ++j) m |= st.thr[j >> 2][1 << (j & 3)];
+  return m;
+}
+
 std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const DevOp* ops, int npool, bool batch,
                             int rb) {
   if (!batch && npool > kJitMaxCoef) return std::string();  // beyond the kernel-parameter space: interpreter
@@ -214,6 +223,7 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
   // the wide passes exist only as compiled kernels with their offsets baked in
   const bool bake = rb != kRegBits || env_int("VQC_JIT_BAKE", 1) != 0;
   const bool async = !batch && jit_extra_smem(adj, M, rb) > 0;
+  const bool warp_local = env_int("VQC_JIT_WARPSYNC", 1) != 0;
   os << "#include \"tile_f32.cuh\"\n"
      << "using namespace vqc;\nusing namespace vqc::f32t;\n";
   if (!batch) {
@@ -287,8 +297,13 @@ std::string jit_pass_source(int M, bool adj, const DevStageF* st, int nst, const
     // the first stage of an asynchronous pass read its input from the buffer it
     // now writes (in the next stage's layout): every read must be done first
     if (async && s == 0 && nst > 1) os << "    __syncthreads();\n";
+    // a CTA barrier only where the warp index moves to other tile bits (the
+    // last stage: against the next tile's first stage)
+    const bool cta = async || !warp_local ||
+                     warp_tile_bits(st[s], M - rb) != warp_tile_bits(st[(s + 1) % nst], M - rb);
     if (bake)
-      os << "    stage_store_k<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w, swm, gdep);\n  }\n";
+      os << "    stage_store_k<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w, swm, gdep, "
+         << (cta ? "true" : "false") << ");\n  }\n";
     else
       os << "    stage_store<M, ADJ>(x, S, " << (s == nst - 1 ? "true" : "false") << ", v, w);\n  }\n";
   }
@@ -405,8 +420,8 @@ int jit_pass_kernels(int M, bool adj, const std::vector<JitPassRef>& refs, std::
                      bool compile, int rb) {
   out.assign(refs.size(), nullptr);
   if (!jit_available()) return VQC_OK;
-  const int flags[7] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M, rb), M,
-                        batch ? 0 : (int)jit_extra_smem(adj, M, rb), batch ? 1 : 0, rb};
+  const int flags[8] = {env_int("VQC_JIT_BAKE", 1), env_int("VQC_JIT_L2PF", 1), jit_min_blocks(adj, M, rb), M,
+                        batch ? 0 : (int)jit_extra_smem(adj, M, rb), batch ? 1 : 0, rb, env_int("VQC_JIT_WARPSYNC", 1)};
   std::vector<std::pair<uint64_t, uint64_t>> keys(refs.size());
   std::vector<size_t> miss;
   {

@@ -876,10 +876,14 @@ __device__ __forceinline__ void stage_load_k(const TileCtx<M, ADJ, RB>& x, const
     }
   }
 }
+// cta = false: the next stage (or the next tile's first stage) maps the warp
+// index to the same tile bits as this one, so every pair a thread reads next
+// was stored by its own warp and a warp barrier orders the exchange (a thread
+// stores only the pairs it loaded, so no other warp's reads are overtaken).
 template <int M, bool ADJ, int RB, int NP>
 __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ, RB>& x, const DevStageF* S, bool last,
                                               const Pk (&v)[NP], const Pk (&w)[NP], const uint32_t (&swm)[NP],
-                                              const int64_t (&gdep)[NP]) {
+                                              const int64_t (&gdep)[NP], bool cta = true) {
   if (last) {
     const int64_t g0 = (int64_t)x.base + S->gthr[0][x.tlo] + S->gthr[1][x.thi];
 #pragma unroll
@@ -900,7 +904,10 @@ __device__ __forceinline__ void stage_store_k(const TileCtx<M, ADJ, RB>& x, cons
       if (ADJ) x.sl[a] = make_ulonglong2(w[m].r, w[m].i);
     }
   }
-  __syncthreads();
+  if (cta)
+    __syncthreads();
+  else
+    __syncwarp();
 }
 
 // ----------------------------------------------------------------------------- asynchronous tile copies
