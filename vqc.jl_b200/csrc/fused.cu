@@ -168,9 +168,6 @@ struct PlanPass {
   std::vector<FOp> ops;
   std::vector<PlanStage> stages;
   int nslots = 0;
-  // FP32 body: the tile bits the warp index takes in every stage whose
-  // register set avoids them (consecutive such stages exchange within warps)
-  uint32_t warp_mask = 0;
 };
 
 struct TileConfig {
@@ -280,25 +277,16 @@ static void plan_passes(int n, const TileConfig& tc, bool adj, std::vector<PItem
   }
 }
 
-static bool env_on_fused(const char* name, bool dflt) {
-  const char* v = std::getenv(name);
-  return v && *v ? std::atoi(v) != 0 : dflt;
-}
-
 // Conflict check of a register-bit set for the shared-memory swizzle.
 // FP64: 16-byte amplitudes, quarter-warps over the tile swizzle Swz<double>;
 // FP32: 8-byte amplitudes, half-warps over Swz<float>.  Packed FP32: 16-byte
 // pairs, the lowest three thread bits (tile bits outside rs, ascending) must
 // fall in distinct classes of the pair swizzle, class = (tile bit - 1) mod 3.
-static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype, bool packed, uint32_t wmask = 0) {
+static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype, bool packed) {
   if (packed) {
-    // the lowest three thread bits: the lowest tile bits outside the register
-    // set (and outside the warp bits when the stage keeps them)
-    for (int b : rs)
-      if (wmask >> b & 1) wmask = 0;
     int seen = 0, k = 0;
     for (int b = 1; b < M && k < 3; ++b) {
-      if (std::find(rs.begin(), rs.end(), b) != rs.end() || (wmask >> b & 1)) continue;
+      if (std::find(rs.begin(), rs.end(), b) != rs.end()) continue;
       const int res = (b - 1) % 3;
       if (seen >> res & 1) return false;
       seen |= 1 << res;
@@ -330,34 +318,10 @@ static bool rs_conflict_free(const std::vector<int>& rs, int M, int dtype, bool 
 static void plan_stages(PlanPass& p, int M, int dtype, bool packed, int rb = kRegBits) {
   const bool lane0 = packed;
   p.stages.clear();
-  p.warp_mask = 0;
   std::map<int, int> tbit;  // global qubit -> tile bit
   for (int b = 0; b < (int)p.tile_q.size(); ++b) tbit[p.tile_q[b]] = b;
-  auto need_of = [&](const FOp& f) {
-    std::vector<int> need;
-    if (f.kind == kOpU1) need = {tbit[f.tq[0]]};
-    if (f.kind == kOpU2) need = {tbit[f.tq[0]], tbit[f.tq[1]]};
-    return need;
-  };
-  // FP32: the warp index's tile bits, fixed for the pass where the stages
-  // allow: the tile bits the fewest ops need in registers (the highest on a
-  // tie), above the four always-resident low qubits (they stay lane bits, so
-  // a warp's HBM accesses cover whole 128-byte runs).  Stages are formed
-  // without them while any op can go; the ops that need them then share as
-  // few stages as possible.
-  const int nwb = (packed && env_on_fused("VQC_JIT_WARPSYNC", true)) ? std::max(0, M - rb - 5) : 0;
-  if (nwb > 0) {
-    std::vector<int> cnt(M, 0);
-    for (const FOp& f : p.ops)
-      for (int b : need_of(f)) ++cnt[b];
-    std::vector<int> bits;
-    for (int b = std::min(4, M); b < M; ++b) bits.push_back(b);
-    std::stable_sort(bits.begin(), bits.end(), [&](int a, int b) { return cnt[a] != cnt[b] ? cnt[a] < cnt[b] : a > b; });
-    for (int i = 0; i < nwb && i < (int)bits.size(); ++i) p.warp_mask |= 1u << bits[i];
-  }
   std::vector<int> pending(p.ops.size());
   for (size_t i = 0; i < pending.size(); ++i) pending[i] = (int)i;
-  bool allow_w = p.warp_mask == 0;
   while (!pending.empty()) {
     PlanStage st;
     uint64_t blocked = 0;
@@ -371,13 +335,13 @@ static void plan_stages(PlanPass& p, int M, int dtype, bool packed, int rb = kRe
         rest.push_back(oi);
         continue;
       }
-      std::vector<int> need = need_of(f);
-      bool w = false;
-      for (int b : need) w = w || (p.warp_mask >> b & 1);
+      std::vector<int> need;
+      if (f.kind == kOpU1) need = {tbit[f.tq[0]]};
+      if (f.kind == kOpU2) need = {tbit[f.tq[0]], tbit[f.tq[1]]};
       std::vector<int> u = rs;
       for (int b : need)
         if (std::find(u.begin(), u.end(), b) == u.end()) u.push_back(b);
-      if ((int)u.size() <= rb && (allow_w || !w)) {
+      if ((int)u.size() <= rb) {
         rs = u;
         st.ops.push_back(oi);
       } else {
@@ -385,11 +349,6 @@ static void plan_stages(PlanPass& p, int M, int dtype, bool packed, int rb = kRe
         rest.push_back(oi);
       }
     }
-    if (st.ops.empty()) {  // every op left needs a warp bit: a stage with them
-      allow_w = true;
-      continue;
-    }
-    allow_w = p.warp_mask == 0;
     // fill the register set to 4 bits: control bits of the stage's ops first
     std::vector<int> cand;
     for (int oi : st.ops) {
@@ -401,13 +360,8 @@ static void plan_stages(PlanPass& p, int M, int dtype, bool packed, int rb = kRe
             cand.push_back(b);
         }
     }
-    bool stage_w = false;
-    for (int b : rs) stage_w = stage_w || (p.warp_mask >> b & 1);
-    const uint32_t wkeep = stage_w ? 0u : p.warp_mask;  // fill bits keep clear of the warp bits
-    cand.erase(std::remove_if(cand.begin(), cand.end(), [&](int b) { return (wkeep >> b & 1) != 0; }), cand.end());
     for (int b = 0; b < M; ++b)
-      if (std::find(rs.begin(), rs.end(), b) == rs.end() && std::find(cand.begin(), cand.end(), b) == cand.end() &&
-          !(wkeep >> b & 1))
+      if (std::find(rs.begin(), rs.end(), b) == rs.end() && std::find(cand.begin(), cand.end(), b) == cand.end())
         cand.push_back(b);
     const int need_more = rb - (int)rs.size();
     std::vector<int> best;
@@ -420,7 +374,7 @@ static void plan_stages(PlanPass& p, int M, int dtype, bool packed, int rb = kRe
         if (mask >> i & 1) t.push_back(cand[i]);
       std::sort(t.begin(), t.end());
       if (best.empty()) best = t;
-      if (rs_conflict_free(t, M, dtype, packed, wkeep)) {
+      if (rs_conflict_free(t, M, dtype, packed)) {
         best = t;
         found = true;
       }
@@ -585,15 +539,9 @@ static void stage_f32(const PlanPass& p, const PlanStage& st, int M, int n, uint
     dep[j] = t;
     s.dep[j] = t;
   }
-  // thread bits: the tile bits outside the register set, ascending; when the
-  // stage keeps the pass's warp bits out of its registers they go last (the
-  // warp index), so such stages exchange within warps
   std::vector<int> thr;
-  const uint32_t wkeep = (rsmask & p.warp_mask) ? 0u : p.warp_mask;
   for (int b = 0; b < M; ++b)
-    if (!(rsmask >> b & 1) && !(wkeep >> b & 1)) thr.push_back(b);
-  for (int b = 0; b < M; ++b)
-    if (wkeep >> b & 1) thr.push_back(b);
+    if (!(rsmask >> b & 1)) thr.push_back(b);
   auto gq = [&](uint32_t t) {
     int64_t g = 0;
     for (int b = 0; b < M; ++b)
