@@ -620,8 +620,9 @@ def serve_record(local_rank, requests=2000, rates=(500.0, 1000.0, 2000.0, 4000.0
         return {"rate_offered": rate, "requests": count, "throughput": count / makespan,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}
 
-    # warm-up (kernel loads, allocator pools)
-    stream(200.0, min(200, nreq))
+    # warm-up (kernel loads, allocator pools, and the batch kernels compiled
+    # per pass structure: most of the workload's structures appear in it)
+    stream(400.0, min(800, nreq))
     results = [stream(float(r), nreq) for r in rates]
     # the baseline's warm-up: one request of every (size, kind), so that the
     # kernels compiled per structure (the Pauli passes of 2^20+ amplitudes) are
